@@ -1,0 +1,167 @@
+/*
+ * lsvd.h -- C ABI of liblsvd_b200.so, the B200 (sm_100a) implementation of the
+ * dense rotor-schedule hot path of the Rust crate `lie_cliffalg_analog_svd`
+ * v0.44.0: polar/Jacobi SVD, the n<=4 micro kernels, Newton-Schulz polar,
+ * Phase-JADE joint diagonalisation, the rotor stream that the
+ * phase-schedule-v1 compiler consumes, and the SVD diagnostics.
+ *
+ * Conventions (all entry points):
+ *   - matrices are dense row-major f64 (`ndarray::Array2<f64>` standard
+ *     layout), with an explicit leading dimension where one is taken;
+ *   - pointers are HOST pointers unless `LSVD_DEVICE_POINTERS` is set in
+ *     `flags`, in which case every array argument (except the per-matrix
+ *     size array `n` of batched calls, which is always host memory) is
+ *     device memory on the context's device;
+ *   - every entry point returns an `lsvd_status`; nothing traps, throws
+ *     across the ABI or exits; the reference's `assert!` panics on bad
+ *     shapes become `LSVD_BAD_SHAPE`;
+ *   - a context owns one CUDA stream and its workspaces and is not
+ *     thread-safe: use one context per host thread;
+ *   - host-pointer calls are synchronous; device-pointer calls with
+ *     `LSVD_ASYNC` return after enqueueing on the context's stream.
+ */
+#ifndef LSVD_H
+#define LSVD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSVD_API __attribute__((visibility("default")))
+
+typedef enum lsvd_status {
+    LSVD_OK = 0,
+    LSVD_NOT_CONVERGED = 1,   /* an iteration cap was hit; results are returned */
+    LSVD_NONFINITE_INPUT = 2, /* NaN/Inf in the input; outputs are NaN */
+    LSVD_BAD_SHAPE = 3,       /* the reference would panic (assert!) */
+    LSVD_BAD_ARGUMENT = 4,    /* NULL pointer, bad leading dimension, bad flag */
+    LSVD_CUDA_ERROR = 5,      /* see lsvd_context_last_error */
+    LSVD_OUT_OF_MEMORY = 6,
+    LSVD_ROTOR_OVERFLOW = 7,  /* rotor buffer too small; count holds the need */
+    LSVD_NO_DEVICE = 8,
+    LSVD_UNSUPPORTED = 9      /* size or option outside what this build handles */
+} lsvd_status;
+
+/* flags */
+#define LSVD_DEVICE_POINTERS 0x1u /* array arguments are device pointers */
+#define LSVD_WANT_DIAG 0x2u       /* fill rel_recon / orth_u / orth_v in lsvd_diag */
+#define LSVD_ASYNC 0x4u           /* with device pointers: do not synchronise */
+
+/* per-matrix outcome bits (lsvd_diag.flags) */
+#define LSVD_MAT_POLAR_UNTRUSTED 0x01 /* newton_schulz_polar returned ok=false */
+#define LSVD_MAT_REPAIRED 0x02        /* U rebuilt by repair_left_basis_from_right */
+#define LSVD_MAT_NS_CAP 0x04          /* 120 Newton-Schulz iterations without convergence */
+#define LSVD_MAT_JACOBI_CAP 0x08      /* Jacobi sweep cap hit */
+#define LSVD_MAT_MICRO_FALLBACK 0x10  /* LieSvdMicro escalated to LieSvdSmall */
+#define LSVD_MAT_NONFINITE 0x20       /* non-finite input */
+#define LSVD_MAT_ROTOR_OVERFLOW 0x40  /* rotor stream truncated */
+#define LSVD_MAT_NS_DIVERGED 0x80     /* polar iteration diverged -> MGS(A) */
+
+/* route (lsvd_diag.route) */
+#define LSVD_ROUTE_MICRO 0
+#define LSVD_ROUTE_SMALL 1
+
+typedef struct lsvd_diag {
+    double rel_recon; /* ||U S Vt - A||_F / ||A||_F      (src/lib.rs:158-159) */
+    double orth_u;    /* ||U^T U - I||_F                  (src/lib.rs:161)     */
+    double orth_v;    /* ||Vt Vt^T - I||_F                (src/lib.rs:162)     */
+    int32_t ns_iters;      /* Newton-Schulz iterations executed */
+    int32_t jacobi_sweeps; /* Jacobi sweeps started */
+    int64_t rotations;     /* accepted plane rotations */
+    int32_t flags;         /* LSVD_MAT_* bits */
+    int32_t route;         /* LSVD_ROUTE_* */
+} lsvd_diag;
+
+/* One accepted plane rotation of the right basis: V <- V G, where G acts on
+ * columns (i, j), i < j, as  v_i' = cos(theta) v_i - sin(theta) v_j,
+ * v_j' = sin(theta) v_i + cos(theta) v_j  (the apply_basis_rotor convention,
+ * src/lie_svd_joint.rs:428-437).  `round` numbers conflict-free layers:
+ * round = sweep * layers_per_sweep + layer. */
+typedef struct lsvd_rotor {
+    uint16_t i;
+    uint16_t j;
+    uint32_t round;
+    double theta;
+} lsvd_rotor;
+
+typedef enum lsvd_precision {
+    LSVD_PREC_FP64 = 0,       /* the reference algorithm in FP64 throughout */
+    LSVD_PREC_MIXED_TF32 = 1, /* TF32 tensor-core bulk + FP64 refinement/cleanup */
+    LSVD_PREC_MIXED_BF16 = 2  /* BF16 tensor-core bulk + FP64 refinement/cleanup */
+} lsvd_precision;
+
+typedef struct lsvd_context lsvd_context;
+
+LSVD_API const char* lsvd_version(void);
+LSVD_API const char* lsvd_status_string(lsvd_status s);
+
+LSVD_API lsvd_status lsvd_context_create(int device, lsvd_context** out);
+LSVD_API lsvd_status lsvd_context_destroy(lsvd_context* ctx);
+/* Use `stream` (a cudaStream_t) instead of the context's own stream. */
+LSVD_API lsvd_status lsvd_context_set_stream(lsvd_context* ctx, void* stream);
+LSVD_API void* lsvd_context_get_stream(lsvd_context* ctx);
+LSVD_API lsvd_status lsvd_synchronize(lsvd_context* ctx);
+LSVD_API const char* lsvd_context_last_error(const lsvd_context* ctx);
+/* Number of kernels this context has launched since creation. */
+LSVD_API int64_t lsvd_context_kernel_launches(const lsvd_context* ctx);
+
+/* ---------------------------------------------------------------- SVD ---- */
+
+/* Replaces LieSvdSmall::solve (src/lie_svd_small.rs:296-323): Newton-Schulz
+ * polar A = QP, P = sym(Q^T A), Jacobi eigensolve of P, U = QV, left-basis
+ * repair.  A n*n (lda), U n*n (ldu), S n (descending), Vt n*n (ldvt).
+ * n in 1..64.  `rotors` (may be NULL) receives the accepted rotation stream
+ * of the eigensolve, up to rotor_cap entries; *rotor_count gets the number
+ * produced.  `perm` (may be NULL, n int32) receives the sort permutation:
+ * column k of the returned V is column perm[k] of the rotor-stream product. */
+LSVD_API lsvd_status lsvd_small_solve_f64(lsvd_context* ctx, int64_t n, const double* A,
+                                          int64_t lda, double* U, int64_t ldu, double* S,
+                                          double* Vt, int64_t ldvt, lsvd_diag* diag,
+                                          lsvd_rotor* rotors, int64_t rotor_cap,
+                                          int64_t* rotor_count, int32_t* perm, uint32_t flags);
+
+/* Replaces LieSvdMicro::solve (src/lie_svd_micro.rs:21-52), n in 0..4. */
+LSVD_API lsvd_status lsvd_micro_solve_f64(lsvd_context* ctx, int64_t n, const double* A,
+                                          int64_t lda, double* U, int64_t ldu, double* S,
+                                          double* Vt, int64_t ldvt, lsvd_diag* diag,
+                                          uint32_t flags);
+
+/* Replaces LieSvdSmall::solve_rectangular (src/lie_svd_small.rs:340-360):
+ * thin SVD of an m*d matrix via QR reduction; k = min(m, d);
+ * U m*k, S k, Vt k*d.  min(m, d) in 1..64. */
+LSVD_API lsvd_status lsvd_small_solve_rectangular_f64(lsvd_context* ctx, int64_t m, int64_t d,
+                                                      const double* A, int64_t lda, double* U,
+                                                      int64_t ldu, double* S, double* Vt,
+                                                      int64_t ldvt, lsvd_diag* diag,
+                                                      uint32_t flags);
+
+/* Batched uneven SVD (no reference counterpart; each matrix takes the route
+ * LieSvd::solve's exact tiers take: LieSvdMicro for n<=4
+ * (src/lie_svd_adaptive.rs:105-106), LieSvdSmall otherwise).
+ * Matrix t is n[t]*n[t] (n[t] in 1..64); A, U and Vt hold the matrices back
+ * to back (row-major, no padding), S the singular values back to back.
+ * `n` is host memory.  `diags` (may be NULL) gets one lsvd_diag per matrix.
+ * The per-size schedule (sort, work items, tile shapes) is planned once per
+ * distinct `n` array and cached in the context together with a captured CUDA
+ * graph. */
+LSVD_API lsvd_status lsvd_svd_batched_f64(lsvd_context* ctx, int64_t count, const int32_t* n,
+                                          const double* A, double* U, double* S, double* Vt,
+                                          lsvd_diag* diags, lsvd_precision precision,
+                                          uint32_t flags);
+
+/* Replaces metrics::compute (src/lib.rs:149-194) for one matrix (general
+ * thin shape: A m*d, U m*k, S k, Vt k*d).  out[0..4] = rel_recon, orth_u,
+ * orth_v, sigma_max_rel, sigma_tail_rel (NaN when sigma_ref is NULL). */
+LSVD_API lsvd_status lsvd_metrics_f64(lsvd_context* ctx, int64_t m, int64_t d, int64_t k,
+                                      const double* A, const double* U, const double* S,
+                                      const double* Vt, const double* sigma_ref, double* out,
+                                      uint32_t flags);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LSVD_H */

@@ -1,0 +1,14 @@
+"""B200-native (sm_100a) implementation of the dense rotor-schedule hot path of
+the Rust crate ``lie_cliffalg_analog_svd`` v0.44.0.
+
+The compute lives in ``_lib/liblsvd_b200.so`` (CUDA, C ABI in
+``include/lsvd.h``); this package is the Python host mirror of the reference
+API over that ABI.  Importing the package does not load the library;
+the first call does, and fails loudly if it was not built.
+"""
+from .api import (Context, LieSvd, LieSvdMicro, LieSvdSmall, SmallResult, SvdMetrics,  # noqa: F401
+                  default_context, metrics, packed_offsets, svd_batched, unpack)
+from ._lib import LsvdError  # noqa: F401
+
+__all__ = ["Context", "LieSvd", "LieSvdMicro", "LieSvdSmall", "SmallResult", "SvdMetrics",
+           "default_context", "metrics", "packed_offsets", "svd_batched", "unpack", "LsvdError"]

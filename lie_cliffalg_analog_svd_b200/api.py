@@ -1,0 +1,295 @@
+"""Python host mirror of the reference's API for the hot path, over the C ABI.
+
+Names, argument meaning and error behaviour follow the Rust crate
+``lie_cliffalg_analog_svd`` v0.44.0:
+
+* ``LieSvdSmall.solve(a) -> (U, sigma, Vt)``      src/lie_svd_small.rs:296
+* ``LieSvdSmall.solve_rectangular(a)``            src/lie_svd_small.rs:340
+* ``LieSvdMicro.solve(a)``                        src/lie_svd_micro.rs:21
+* ``LieSvd.solve(a)`` -- the exact tiers of the dispatcher: Micro for n <= 4
+  (src/lie_svd_adaptive.rs:105-106), Small otherwise
+* ``metrics.compute(a, u, sigma, vt, sigma_ref)``  src/lib.rs:149
+* ``svd_batched(ns, a)`` -- the batched entry (no reference counterpart)
+
+Where the reference panics (``assert!``) these raise ``LsvdError`` with status
+``BAD_SHAPE``.  Every call runs on the GPU through ``liblsvd_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _check(lib, ctx_ptr, status: int, what: str):
+    if status in (L.OK,):
+        return
+    msg = lib.lsvd_status_string(status).decode()
+    detail = lib.lsvd_context_last_error(ctx_ptr).decode() if ctx_ptr else ""
+    raise L.LsvdError(status, f"{what}: {msg} {detail}".strip())
+
+
+class Context:
+    """One ``lsvd_context`` (device, CUDA stream, workspaces, plan cache)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = L.load()
+        h = C.c_void_p()
+        st = self.lib.lsvd_context_create(device, C.byref(h))
+        if st != L.OK:
+            raise L.LsvdError(st, f"lsvd_context_create: {self.lib.lsvd_status_string(st).decode()}")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            self.lib.lsvd_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int):
+        _check(self.lib, self.handle, self.lib.lsvd_context_set_stream(self.handle, C.c_void_p(stream_handle)),
+               "set_stream")
+
+    @property
+    def stream(self) -> int:
+        return self.lib.lsvd_context_get_stream(self.handle) or 0
+
+    def synchronize(self):
+        _check(self.lib, self.handle, self.lib.lsvd_synchronize(self.handle), "synchronize")
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.lsvd_context_kernel_launches(self.handle))
+
+
+_tls = threading.local()
+
+
+def default_context(device: int = 0) -> Context:
+    """Per-thread default context (a context is not thread-safe)."""
+    ctxs = getattr(_tls, "ctxs", None)
+    if ctxs is None:
+        ctxs = _tls.ctxs = {}
+    if device not in ctxs:
+        ctxs[device] = Context(device)
+    return ctxs[device]
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def _diag_dict(d: L.Diag) -> dict:
+    return {k: getattr(d, k) for k, _ in L.Diag._fields_}
+
+
+@dataclass
+class SmallResult:
+    u: np.ndarray
+    sigma: np.ndarray
+    vt: np.ndarray
+    diag: dict
+    rotors: np.ndarray | None
+    perm: np.ndarray
+
+
+class LieSvdSmall:
+    """``LieSvdSmall`` (src/lie_svd_small.rs:291-361) on the GPU."""
+
+    @staticmethod
+    def solve(a, ctx: Context | None = None):
+        """Full SVD ``(U, sigma, Vt)`` of a square matrix (n <= 64)."""
+        r = LieSvdSmall.solve_full(a, ctx=ctx)
+        return r.u, r.sigma, r.vt
+
+    @staticmethod
+    def solve_full(a, ctx: Context | None = None, want_diag: bool = True,
+                   rotor_cap: int = 0) -> SmallResult:
+        """``solve`` plus diagnostics, the sort permutation and (if
+        ``rotor_cap`` > 0) the accepted rotor stream of the eigensolve."""
+        ctx = ctx or default_context()
+        a = _f64(a)
+        if a.ndim != 2 or a.shape[0] != a.shape[1]:
+            raise L.LsvdError(L.BAD_SHAPE, "LieSvdSmall::solve: matrix must be square N×N")
+        n = a.shape[0]
+        u = np.empty((n, n)); s = np.empty(n); vt = np.empty((n, n))
+        d = L.Diag()
+        perm = np.empty(n, dtype=np.int32)
+        rot = np.empty(max(rotor_cap, 1), dtype=L.ROTOR_DTYPE) if rotor_cap else None
+        cnt = C.c_int64(0)
+        st = ctx.lib.lsvd_small_solve_f64(
+            ctx.handle, n, _ptr(a), n, _ptr(u), n, _ptr(s), _ptr(vt), n, C.byref(d),
+            _ptr(rot) if rot is not None else None, rotor_cap, C.byref(cnt), _ptr(perm),
+            L.WANT_DIAG if want_diag else 0)
+        if st not in (L.OK, L.NOT_CONVERGED, L.NONFINITE_INPUT, L.ROTOR_OVERFLOW):
+            _check(ctx.lib, ctx.handle, st, "LieSvdSmall::solve")
+        dd = _diag_dict(d)
+        dd["status"] = st
+        dd["rotor_count"] = cnt.value
+        return SmallResult(u, s, vt, dd, rot[:min(cnt.value, rotor_cap)] if rot is not None else None,
+                           perm)
+
+    @staticmethod
+    def solve_rectangular(a, ctx: Context | None = None):
+        """Thin SVD of an m×d matrix (min(m, d) <= 64): U m×k, sigma k, Vt k×d."""
+        ctx = ctx or default_context()
+        a = _f64(a)
+        if a.ndim != 2 or a.shape[0] == 0 or a.shape[1] == 0:
+            raise L.LsvdError(L.BAD_SHAPE, "LieSvdSmall::solve_rectangular: empty input")
+        m, d = a.shape
+        k = min(m, d)
+        u = np.empty((m, k)); s = np.empty(k); vt = np.empty((k, d))
+        st = ctx.lib.lsvd_small_solve_rectangular_f64(ctx.handle, m, d, _ptr(a), d, _ptr(u), k,
+                                                      _ptr(s), _ptr(vt), d, None, 0)
+        if st not in (L.OK, L.NOT_CONVERGED):
+            _check(ctx.lib, ctx.handle, st, "LieSvdSmall::solve_rectangular")
+        return u, s, vt
+
+
+class LieSvdMicro:
+    """``LieSvdMicro`` (src/lie_svd_micro.rs:17-53) on the GPU."""
+
+    @staticmethod
+    def solve(a, ctx: Context | None = None, diag: bool = False):
+        ctx = ctx or default_context()
+        a = _f64(a)
+        n = a.shape[0]
+        if a.ndim != 2 or a.shape[1] != n:
+            raise L.LsvdError(L.BAD_SHAPE, "LieSvdMicro: matrix must be square")
+        if n > 4:
+            raise L.LsvdError(L.BAD_SHAPE, "LieSvdMicro only supports N <= 4")
+        u = np.empty((n, n)); s = np.empty(n); vt = np.empty((n, n))
+        d = L.Diag()
+        if n:
+            st = ctx.lib.lsvd_micro_solve_f64(ctx.handle, n, _ptr(a), n, _ptr(u), n, _ptr(s),
+                                              _ptr(vt), n, C.byref(d), L.WANT_DIAG)
+            if st not in (L.OK, L.NONFINITE_INPUT):
+                _check(ctx.lib, ctx.handle, st, "LieSvdMicro::solve")
+        return (u, s, vt, _diag_dict(d)) if diag else (u, s, vt)
+
+
+class LieSvd:
+    """The exact tiers of ``LieSvd::solve`` (src/lie_svd.rs:49): Micro for
+    n <= MICRO_MAX_N = 4, Small otherwise.  The adaptive triage that may send
+    structured inputs to the PhaseFlow/CoreFlow research routes is not part of
+    this library."""
+
+    MICRO_MAX_N = 4
+
+    @staticmethod
+    def solve(a, ctx: Context | None = None):
+        a = _f64(a)
+        if a.shape[0] <= LieSvd.MICRO_MAX_N:
+            return LieSvdMicro.solve(a, ctx=ctx)
+        return LieSvdSmall.solve(a, ctx=ctx)
+
+
+@dataclass
+class SvdMetrics:
+    rel_recon: float
+    orth_u: float
+    orth_v: float
+    sigma_max_rel: float | None
+    sigma_tail_rel: float | None
+
+
+class metrics:  # noqa: N801 -- mirrors the Rust module name
+    """``metrics::compute`` (src/lib.rs:149-194) on the GPU."""
+
+    @staticmethod
+    def compute(a, u, sigma, vt, sigma_ref=None, ctx: Context | None = None) -> SvdMetrics:
+        ctx = ctx or default_context()
+        a, u, sigma, vt = _f64(a), _f64(u), _f64(sigma), _f64(vt)
+        m, d = a.shape
+        k = sigma.shape[0]
+        ref = _f64(sigma_ref) if sigma_ref is not None else None
+        out = np.empty(5)
+        st = ctx.lib.lsvd_metrics_f64(ctx.handle, m, d, k, _ptr(a), _ptr(u), _ptr(sigma), _ptr(vt),
+                                      _ptr(ref) if ref is not None else None, _ptr(out), 0)
+        _check(ctx.lib, ctx.handle, st, "metrics::compute")
+        return SvdMetrics(out[0], out[1], out[2], None if ref is None else out[3],
+                          None if ref is None else out[4])
+
+
+PRECISIONS = {"fp64": L.PREC_FP64, "tf32": L.PREC_MIXED_TF32, "bf16": L.PREC_MIXED_BF16}
+
+
+def packed_offsets(ns) -> tuple[np.ndarray, np.ndarray]:
+    ns = np.asarray(ns, dtype=np.int64)
+    ao = np.zeros(ns.size + 1, dtype=np.int64)
+    ao[1:] = np.cumsum(ns * ns)
+    so = np.zeros(ns.size + 1, dtype=np.int64)
+    so[1:] = np.cumsum(ns)
+    return ao, so
+
+
+def svd_batched(ns, a, precision: str = "fp64", want_diag: bool = False,
+                ctx: Context | None = None, out=None, device_async: bool = False):
+    """Batched uneven SVD.  ``ns``: int sizes (1..64); ``a``: the matrices
+    back to back, row-major (numpy array on the host, or a CUDA torch tensor
+    for the device-pointer path).  Returns ``(U, S, Vt, diags, status)`` in the
+    same packed layout (torch tensors when ``a`` is a torch tensor)."""
+    ctx = ctx or default_context()
+    ns = np.ascontiguousarray(ns, dtype=np.int32)
+    count = ns.size
+    ao, so = packed_offsets(ns)
+    prec = PRECISIONS[precision]
+    flags = L.WANT_DIAG if want_diag else 0
+    is_torch = type(a).__module__.startswith("torch")
+    if is_torch:
+        import torch
+        assert a.is_cuda and a.dtype == torch.float64 and a.is_contiguous()
+        if out is None:
+            u = torch.empty(int(ao[-1]), dtype=torch.float64, device=a.device)
+            s = torch.empty(int(so[-1]), dtype=torch.float64, device=a.device)
+            vt = torch.empty(int(ao[-1]), dtype=torch.float64, device=a.device)
+            dg = torch.empty(count * C.sizeof(L.Diag) if want_diag else 8, dtype=torch.uint8, device=a.device)
+        else:
+            u, s, vt, dg = out
+        flags |= L.DEVICE_POINTERS | (L.ASYNC if device_async else 0)
+        st = ctx.lib.lsvd_svd_batched_f64(ctx.handle, count, _ptr(ns), C.c_void_p(a.data_ptr()),
+                                          C.c_void_p(u.data_ptr()), C.c_void_p(s.data_ptr()),
+                                          C.c_void_p(vt.data_ptr()),
+                                          C.c_void_p(dg.data_ptr()) if want_diag else None, prec,
+                                          flags)
+        if st not in (L.OK, L.NOT_CONVERGED, L.NONFINITE_INPUT):
+            _check(ctx.lib, ctx.handle, st, "svd_batched")
+        return u, s, vt, (dg if want_diag else None), st
+    a = _f64(a)
+    assert a.size == ao[-1], "packed A has the wrong length for ns"
+    if out is None:
+        u = np.empty(int(ao[-1])); s = np.empty(int(so[-1])); vt = np.empty(int(ao[-1]))
+        dg = np.empty(count, dtype=L.DIAG_DTYPE) if want_diag else None
+    else:
+        u, s, vt, dg = out
+    st = ctx.lib.lsvd_svd_batched_f64(ctx.handle, count, _ptr(ns), _ptr(a), _ptr(u), _ptr(s),
+                                      _ptr(vt), _ptr(dg) if dg is not None else None, prec, flags)
+    if st not in (L.OK, L.NOT_CONVERGED, L.NONFINITE_INPUT):
+        _check(ctx.lib, ctx.handle, st, "svd_batched")
+    return u, s, vt, dg, st
+
+
+def unpack(ns, packed, square: bool = True):
+    """Splits a packed buffer into per-matrix arrays."""
+    ns = np.asarray(ns, dtype=np.int64)
+    ao, so = packed_offsets(ns)
+    off = ao if square else so
+    out = []
+    for t, n in enumerate(ns):
+        blk = packed[off[t]:off[t + 1]]
+        out.append(blk.reshape(n, n) if square else blk)
+    return out

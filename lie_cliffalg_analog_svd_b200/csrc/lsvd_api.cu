@@ -1,0 +1,602 @@
+// lsvd_api.cu -- host side of liblsvd_b200.so: contexts, workspaces, the
+// batched planner (size classes, LPT work items, CUDA-graph capture) and the
+// C ABI declared in include/lsvd.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "lsvd.h"
+#include "lsvd_internal.h"
+#include "lsvd_kernels.cuh"
+
+using namespace lsvd;
+
+// ------------------------------------------------------------ context ----
+
+lsvd_status lsvd_ctx_fail(lsvd_context* ctx, lsvd_status st, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return st;
+}
+
+lsvd_status lsvd_ctx_cuda(lsvd_context* ctx, cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return LSVD_OK;
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return lsvd_ctx_fail(ctx, LSVD_OUT_OF_MEMORY, m);
+    return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, m);
+}
+
+void* DeviceBuffer::get(size_t want, cudaError_t* err) {
+    *err = cudaSuccess;
+    if (want <= bytes) return ptr;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    size_t sz = std::max(want, size_t(256));
+    *err = cudaMalloc(&ptr, sz);
+    if (*err != cudaSuccess) {
+        ptr = nullptr;
+        return nullptr;
+    }
+    bytes = sz;
+    return ptr;
+}
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+extern "C" const char* lsvd_version(void) { return "lsvd_b200 0.1.0 (sm_100a)"; }
+
+extern "C" const char* lsvd_status_string(lsvd_status s) {
+    switch (s) {
+        case LSVD_OK: return "ok";
+        case LSVD_NOT_CONVERGED: return "iteration cap reached";
+        case LSVD_NONFINITE_INPUT: return "non-finite input";
+        case LSVD_BAD_SHAPE: return "bad shape";
+        case LSVD_BAD_ARGUMENT: return "bad argument";
+        case LSVD_CUDA_ERROR: return "CUDA error";
+        case LSVD_OUT_OF_MEMORY: return "out of device memory";
+        case LSVD_ROTOR_OVERFLOW: return "rotor buffer too small";
+        case LSVD_NO_DEVICE: return "no CUDA device";
+        case LSVD_UNSUPPORTED: return "unsupported size or option";
+    }
+    return "unknown status";
+}
+
+extern "C" lsvd_status lsvd_context_create(int device, lsvd_context** out) {
+    if (!out) return LSVD_BAD_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return LSVD_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return LSVD_BAD_ARGUMENT;
+    auto* ctx = new lsvd_context();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return LSVD_CUDA_ERROR;
+    }
+    ctx->own_stream = true;
+    *out = ctx;
+    return LSVD_OK;
+}
+
+lsvd_context::~lsvd_context() {
+    cudaSetDevice(device);
+    for (auto& kv : plans) kv.second.reset();
+    for (auto* b : {&ws_a, &ws_u, &ws_s, &ws_vt, &ws_diag, &ws_misc, &ws_rot})
+        b->release();
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+extern "C" lsvd_status lsvd_context_destroy(lsvd_context* ctx) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    delete ctx;
+    return LSVD_OK;
+}
+
+extern "C" lsvd_status lsvd_context_set_stream(lsvd_context* ctx, void* stream) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    ctx->stream = static_cast<cudaStream_t>(stream);
+    ctx->own_stream = false;
+    for (auto& kv : ctx->plans) kv.second->invalidate_graph();
+    return LSVD_OK;
+}
+
+extern "C" void* lsvd_context_get_stream(lsvd_context* ctx) { return ctx ? ctx->stream : nullptr; }
+
+extern "C" lsvd_status lsvd_synchronize(lsvd_context* ctx) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return lsvd_ctx_cuda(ctx, cudaStreamSynchronize(ctx->stream), "lsvd_synchronize");
+}
+
+extern "C" const char* lsvd_context_last_error(const lsvd_context* ctx) {
+    return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+extern "C" int64_t lsvd_context_kernel_launches(const lsvd_context* ctx) {
+    return ctx ? ctx->launches : -1;
+}
+
+// ---------------------------------------------------------- helpers ----
+
+static bool is_dev(uint32_t flags) { return (flags & LSVD_DEVICE_POINTERS) != 0; }
+
+// 2-D copy of a rows x cols f64 block between (possibly) strided buffers.
+static cudaError_t copy2d(double* dst, int64_t ldd, const double* src, int64_t lds, int64_t rows,
+                          int64_t cols, cudaStream_t s) {
+    if (rows == 0 || cols == 0) return cudaSuccess;
+    return cudaMemcpy2DAsync(dst, size_t(ldd) * 8, src, size_t(lds) * 8, size_t(cols) * 8,
+                             size_t(rows), cudaMemcpyDefault, s);
+}
+
+static int variant_of(int ts, int g) { return (ts == 4 ? 3 : 0) + (g == 16 ? 1 : g == 32 ? 2 : 0); }
+
+// ------------------------------------------------------- single SVD ----
+
+static cudaError_t launch_single(lsvd_context* ctx, const SmallJob& job) {
+    const int n = job.n;
+    const size_t smem = size_t(team_smem_doubles(n)) * sizeof(double);
+    const bool big = n > 32;
+    cudaError_t e;
+    if (big) {
+        e = cudaFuncSetAttribute(single_kernel<4, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+        single_kernel<4, 8><<<1, kCtaThreads, smem, ctx->stream>>>(job);
+    } else {
+        e = cudaFuncSetAttribute(single_kernel<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+        single_kernel<2, 8><<<1, kCtaThreads, smem, ctx->stream>>>(job);
+    }
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
+lsvd_status lsvd_single_small(lsvd_context* ctx, int64_t n, const double* A, int64_t lda,
+                              double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
+                              lsvd_diag* diag, lsvd_rotor* rotors, int64_t rotor_cap,
+                              int64_t* rotor_count, int32_t* perm, uint32_t flags,
+                              int extra_flags) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    if (n < 1 || n > kMaxN)
+        return lsvd_ctx_fail(ctx, n < 1 ? LSVD_BAD_SHAPE : LSVD_UNSUPPORTED,
+                             "LieSvdSmall::solve: n must be in 1..64");
+    if (!A || !U || !S || !Vt || lda < n || ldu < n || ldvt < n || rotor_cap < 0 ||
+        (rotors && rotor_cap > 0 && !rotor_count))
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_small_solve_f64: bad pointer or leading dimension");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const bool dev = is_dev(flags);
+    cudaError_t e;
+    const size_t nn = size_t(n) * size_t(n);
+    double* dA = static_cast<double*>(ctx->ws_a.get(nn * 8, &e));
+    double* dU = e == cudaSuccess ? static_cast<double*>(ctx->ws_u.get(nn * 8, &e)) : nullptr;
+    double* dS = e == cudaSuccess ? static_cast<double*>(ctx->ws_s.get(size_t(n) * 8, &e)) : nullptr;
+    double* dV = e == cudaSuccess ? static_cast<double*>(ctx->ws_vt.get(nn * 8, &e)) : nullptr;
+    char* misc = e == cudaSuccess ? static_cast<char*>(ctx->ws_misc.get(4096, &e)) : nullptr;
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "workspace");
+    lsvd_diag* dDiag = reinterpret_cast<lsvd_diag*>(misc);
+    int64_t* dRotCount = reinterpret_cast<int64_t*>(misc + 256);
+    int32_t* dPerm = reinterpret_cast<int32_t*>(misc + 512);
+    lsvd_rotor* dRot = nullptr;
+    if (rotors && rotor_cap > 0) {
+        if (dev)
+            dRot = rotors;
+        else {
+            dRot = static_cast<lsvd_rotor*>(ctx->ws_rot.get(size_t(rotor_cap) * sizeof(lsvd_rotor), &e));
+            if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "rotor workspace");
+        }
+    }
+    if ((e = copy2d(dA, n, A, lda, n, n, st)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "copy A");
+    SmallJob job;
+    job.n = int(n);
+    job.A = dA;
+    job.lda = n;
+    job.U = dU;
+    job.ldu = n;
+    job.S = dS;
+    job.Vt = dV;
+    job.ldvt = n;
+    job.diag = dDiag;
+    job.rotors = dRot;
+    job.rotor_cap = dRot ? rotor_cap : 0;
+    job.rotor_count = dRotCount;
+    job.perm_out = dPerm;
+    job.want_diag = (flags & LSVD_WANT_DIAG) != 0;
+    job.extra_flags = extra_flags;
+    job.agg = nullptr;
+    if ((e = launch_single(ctx, job)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "single_kernel");
+    if ((e = copy2d(U, ldu, dU, n, n, n, st)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "copy U");
+    if ((e = copy2d(Vt, ldvt, dV, n, n, n, st)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "copy Vt");
+    if ((e = cudaMemcpyAsync(S, dS, size_t(n) * 8, cudaMemcpyDefault, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "copy S");
+    if (perm && (e = cudaMemcpyAsync(perm, dPerm, size_t(n) * 4, cudaMemcpyDefault, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "copy perm");
+    lsvd_diag hdiag;
+    int64_t hcount = 0;
+    if ((e = cudaMemcpyAsync(&hdiag, dDiag, sizeof(hdiag), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&hcount, dRotCount, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "copy diag");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "sync");
+    if (rotors && rotor_cap > 0 && !dev) {
+        const int64_t got = std::min(hcount, rotor_cap);
+        if (got > 0 &&
+            (e = cudaMemcpy(rotors, dRot, size_t(got) * sizeof(lsvd_rotor), cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "copy rotors");
+    }
+    if (rotor_count) {
+        if (dev)
+            cudaMemcpy(rotor_count, &hcount, 8, cudaMemcpyHostToDevice);
+        else
+            *rotor_count = hcount;
+    }
+    if (diag) {
+        if (dev)
+            cudaMemcpy(diag, &hdiag, sizeof(hdiag), cudaMemcpyHostToDevice);
+        else
+            *diag = hdiag;
+    }
+    if (hdiag.flags & LSVD_MAT_NONFINITE) return LSVD_NONFINITE_INPUT;
+    if (hdiag.flags & LSVD_MAT_JACOBI_CAP) return LSVD_NOT_CONVERGED;
+    if (rotors && hcount > rotor_cap) return LSVD_ROTOR_OVERFLOW;
+    return LSVD_OK;
+}
+
+extern "C" lsvd_status lsvd_small_solve_f64(lsvd_context* ctx, int64_t n, const double* A,
+                                            int64_t lda, double* U, int64_t ldu, double* S,
+                                            double* Vt, int64_t ldvt, lsvd_diag* diag,
+                                            lsvd_rotor* rotors, int64_t rotor_cap,
+                                            int64_t* rotor_count, int32_t* perm, uint32_t flags) {
+    return lsvd_single_small(ctx, n, A, lda, U, ldu, S, Vt, ldvt, diag, rotors, rotor_cap,
+                             rotor_count, perm, flags, 0);
+}
+
+extern "C" lsvd_status lsvd_micro_solve_f64(lsvd_context* ctx, int64_t n, const double* A,
+                                            int64_t lda, double* U, int64_t ldu, double* S,
+                                            double* Vt, int64_t ldvt, lsvd_diag* diag,
+                                            uint32_t flags) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    if (n < 0 || n > 4) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "LieSvdMicro only supports N <= 4");
+    if (n == 0) return LSVD_OK;  // empty result, src/lie_svd_micro.rs:27-31
+    if (!A || !U || !S || !Vt || lda < n || ldu < n || ldvt < n)
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_micro_solve_f64: bad pointer or leading dimension");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    cudaError_t e;
+    double* dA = static_cast<double*>(ctx->ws_a.get(16 * 8, &e));
+    double* dU = e == cudaSuccess ? static_cast<double*>(ctx->ws_u.get(16 * 8, &e)) : nullptr;
+    double* dS = e == cudaSuccess ? static_cast<double*>(ctx->ws_s.get(4 * 8, &e)) : nullptr;
+    double* dV = e == cudaSuccess ? static_cast<double*>(ctx->ws_vt.get(16 * 8, &e)) : nullptr;
+    char* misc = e == cudaSuccess ? static_cast<char*>(ctx->ws_misc.get(4096, &e)) : nullptr;
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "workspace");
+    lsvd_diag* dDiag = reinterpret_cast<lsvd_diag*>(misc);
+    int* dFlag = reinterpret_cast<int*>(misc + 1024);
+    int* dAgg = dFlag + 1;
+    if ((e = copy2d(dA, n, A, lda, n, n, st)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "copy A");
+    if ((e = cudaMemsetAsync(dFlag, 0, 8, st)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "memset");
+    micro_single_kernel<<<1, 32, 0, st>>>(int(n), dA, dU, dS, dV, dDiag,
+                                          (flags & LSVD_WANT_DIAG) ? 1 : 0, dFlag, dAgg);
+    ctx->launches++;
+    if ((e = cudaGetLastError()) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "micro kernel");
+    int hflag = 0;
+    if ((e = cudaMemcpyAsync(&hflag, dFlag, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "sync");
+    if (hflag) {  // LieSvdMicro -> LieSvdSmall escalation, src/lie_svd_micro.rs:90-92
+        return lsvd_single_small(ctx, n, A, lda, U, ldu, S, Vt, ldvt, diag, nullptr, 0, nullptr,
+                                 nullptr, flags, LSVD_MAT_MICRO_FALLBACK);
+    }
+    if ((e = copy2d(U, ldu, dU, n, n, n, st)) != cudaSuccess ||
+        (e = copy2d(Vt, ldvt, dV, n, n, n, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(S, dS, size_t(n) * 8, cudaMemcpyDefault, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "copy out");
+    lsvd_diag hdiag;
+    if ((e = cudaMemcpyAsync(&hdiag, dDiag, sizeof(hdiag), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "sync");
+    if (diag) {
+        if (is_dev(flags))
+            cudaMemcpy(diag, &hdiag, sizeof(hdiag), cudaMemcpyHostToDevice);
+        else
+            *diag = hdiag;
+    }
+    return (hdiag.flags & LSVD_MAT_NONFINITE) ? LSVD_NONFINITE_INPUT : LSVD_OK;
+}
+
+// ------------------------------------------------------------ batched ----
+
+// Default size classes (n ranges, team shape, tile variant).  The autotuner
+// (lsvd_autotune.cu) may override the shape per class.
+static const int kClassHi[kMaxClasses] = {4, 8, 16, 24, 32, 48, 64, 64};
+
+int lsvd_class_of(int n) {
+    for (int c = 0; c < kMaxClasses; ++c)
+        if (n <= kClassHi[c]) return c;
+    return kMaxClasses - 1;
+}
+
+static const ClassShape kDefaultShapes[kMaxClasses] = {
+    {0, 2, 8, 64},  // micro: thread per matrix, up to 256 per item
+    {1, 2, 8, 2},   // 5..8
+    {1, 2, 16, 1},  // 9..16
+    {2, 2, 8, 1},   // 17..24
+    {2, 4, 8, 1},   // 25..32
+    {8, 4, 8, 1},   // 33..48
+    {8, 4, 8, 1},   // 49..64
+    {8, 4, 8, 1},
+};
+
+ClassShape lsvd_default_shape(int cls) { return kDefaultShapes[cls]; }
+
+BatchPlan::~BatchPlan() {
+    invalidate_graph();
+    for (auto* b : {&d_meta, &d_scratch, &d_a, &d_u, &d_s, &d_vt, &d_diag}) b->release();
+}
+
+void BatchPlan::invalidate_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    bound_key.clear();
+}
+
+static uint64_t hash_ns(int64_t count, const int32_t* n) {
+    uint64_t h = 1469598103934665603ull ^ uint64_t(count);
+    for (int64_t i = 0; i < count; ++i) {
+        h ^= uint64_t(uint32_t(n[i]));
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+// Builds the LPT schedule: matrices sorted by n descending, grouped into work
+// items of one size class each.
+static lsvd_status build_plan(lsvd_context* ctx, int64_t count, const int32_t* n,
+                              const ClassShape* shapes, BatchPlan& P) {
+    P.count = count;
+    P.ns.assign(n, n + count);
+    std::vector<int32_t> perm(static_cast<size_t>(count));
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) { return n[a] > n[b]; });
+    std::vector<int64_t> aoff(static_cast<size_t>(count)), soff(static_cast<size_t>(count));
+    int64_t ao = 0, so = 0;
+    for (int64_t t = 0; t < count; ++t) {
+        aoff[size_t(t)] = ao;
+        soff[size_t(t)] = so;
+        ao += int64_t(n[t]) * n[t];
+        so += n[t];
+    }
+    P.a_elems = ao;
+    P.s_elems = so;
+    std::vector<Item> items;
+    int max_smem = 0;
+    for (int c = 0; c < kMaxClasses; ++c) {
+        const ClassShape& s = shapes[c];
+        ClassCfg& cfg = P.cls[c];
+        cfg.nwarps = s.nwarps;
+        cfg.variant = variant_of(s.ts, s.g);
+        const int lo = c == 0 ? 1 : kClassHi[c - 1] + 1;
+        const int hi = kClassHi[c];
+        cfg.slice = s.nwarps ? team_smem_doubles(hi) : 0;
+        if (lo > hi) continue;
+    }
+    size_t i = 0;
+    while (i < perm.size()) {
+        const int c = lsvd_class_of(n[perm[i]]);
+        size_t j = i;
+        while (j < perm.size() && lsvd_class_of(n[perm[j]]) == c) ++j;
+        const ClassShape& s = shapes[c];
+        int per_item;
+        if (s.nwarps == 0) {
+            per_item = kCtaThreads;
+        } else {
+            const int teams = kCtaThreads / (32 * s.nwarps);
+            per_item = teams * std::max(1, s.per_team);
+            max_smem = std::max(max_smem, teams * P.cls[c].slice * 8);
+        }
+        for (size_t k = i; k < j; k += size_t(per_item)) {
+            Item it;
+            it.cls = c;
+            it.first = int(k);
+            it.count = int(std::min(j - k, size_t(per_item)));
+            it.pad_ = 0;
+            items.push_back(it);
+        }
+        i = j;
+    }
+    P.n_items = int(items.size());
+    P.smem_bytes = max_smem;
+    // metadata in one device allocation: n | aoff | soff | perm | items
+    const size_t b_n = size_t(count) * 4, b_off = size_t(count) * 8;
+    const size_t b_items = items.size() * sizeof(Item);
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t total = al(b_n) + 2 * al(b_off) + al(b_n) + al(b_items);
+    cudaError_t e;
+    char* base = static_cast<char*>(P.d_meta.get(total, &e));
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "plan metadata");
+    size_t off = 0;
+    P.m_n = reinterpret_cast<int32_t*>(base + off); off += al(b_n);
+    P.m_aoff = reinterpret_cast<int64_t*>(base + off); off += al(b_off);
+    P.m_soff = reinterpret_cast<int64_t*>(base + off); off += al(b_off);
+    P.m_perm = reinterpret_cast<int32_t*>(base + off); off += al(b_n);
+    P.m_items = reinterpret_cast<Item*>(base + off);
+    cudaStream_t st = ctx->stream;
+    if ((e = cudaMemcpyAsync(P.m_n, n, b_n, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(P.m_aoff, aoff.data(), b_off, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(P.m_soff, soff.data(), b_off, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(P.m_perm, perm.data(), b_n, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (b_items && (e = cudaMemcpyAsync(P.m_items, items.data(), b_items, cudaMemcpyHostToDevice, st)) != cudaSuccess))
+        return lsvd_ctx_cuda(ctx, e, "plan upload");
+    // scratch: head | fb_count | agg_flags | pad | fb_list[count]
+    char* sc = static_cast<char*>(P.d_scratch.get(256 + size_t(count) * 4, &e));
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "plan scratch");
+    P.s_head = reinterpret_cast<int*>(sc);
+    P.s_fb_count = P.s_head + 1;
+    P.s_agg = P.s_head + 2;
+    P.s_fb_list = reinterpret_cast<int32_t*>(sc + 256);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "plan sync");
+    return LSVD_OK;
+}
+
+static cudaError_t enqueue_plan(lsvd_context* ctx, BatchPlan& P, const double* A, double* U,
+                                double* S, double* Vt, lsvd_diag* diag, bool want_diag) {
+    cudaStream_t st = ctx->stream;
+    BatchArgs a;
+    a.n = P.m_n;
+    a.aoff = P.m_aoff;
+    a.soff = P.m_soff;
+    a.perm = P.m_perm;
+    a.A = A;
+    a.U = U;
+    a.S = S;
+    a.Vt = Vt;
+    a.diag = diag;
+    a.items = P.m_items;
+    a.n_items = P.n_items;
+    a.want_diag = want_diag ? 1 : 0;
+    a.head = P.s_head;
+    a.fb_count = P.s_fb_count;
+    a.fb_list = P.s_fb_list;
+    a.agg_flags = P.s_agg;
+    for (int c = 0; c < kMaxClasses; ++c) a.cls[c] = P.cls[c];
+    cudaError_t e = cudaMemsetAsync(P.s_head, 0, 16, st);
+    if (e != cudaSuccess) return e;
+    const int smem = std::max(P.smem_bytes, 16);
+    const int grid = std::max(1, std::min(P.n_items, 2 * ctx->num_sms));
+    batched_kernel<<<grid, kCtaThreads, smem, st>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int fsmem = team_smem_doubles(4) * 8;
+    fallback_kernel<<<std::max(1, std::min(ctx->num_sms, int(P.count))), kCtaThreads, fsmem, st>>>(a);
+    return cudaGetLastError();
+}
+
+lsvd_status lsvd_run_plan(lsvd_context* ctx, BatchPlan& P, const double* A, double* U, double* S,
+                          double* Vt, lsvd_diag* diag, bool want_diag, bool use_graph) {
+    cudaError_t e = cudaFuncSetAttribute(batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         std::max(P.smem_bytes, 16));
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "smem attribute");
+    if (!use_graph) {
+        if ((e = enqueue_plan(ctx, P, A, U, S, Vt, diag, want_diag)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "batched launch");
+        ctx->launches += 2;
+        return LSVD_OK;
+    }
+    char key[160];
+    std::snprintf(key, sizeof(key), "%p|%p|%p|%p|%p|%d|%p", (const void*)A, (void*)U, (void*)S,
+                  (void*)Vt, (void*)diag, int(want_diag), (void*)ctx->stream);
+    if (!P.graph_exec || P.bound_key != key) {
+        P.invalidate_graph();
+        cudaGraph_t g;
+        if ((e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "begin capture");
+        cudaError_t e2 = enqueue_plan(ctx, P, A, U, S, Vt, diag, want_diag);
+        e = cudaStreamEndCapture(ctx->stream, &g);
+        if (e2 != cudaSuccess) return lsvd_ctx_cuda(ctx, e2, "capture batched");
+        if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "end capture");
+        e = cudaGraphInstantiate(&P.graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            P.graph_exec = nullptr;
+            return lsvd_ctx_cuda(ctx, e, "graph instantiate");
+        }
+        P.bound_key = key;
+    }
+    if ((e = cudaGraphLaunch(P.graph_exec, ctx->stream)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "graph launch");
+    ctx->launches += 2;
+    return LSVD_OK;
+}
+
+BatchPlan* lsvd_get_plan(lsvd_context* ctx, int64_t count, const int32_t* n, lsvd_precision prec,
+                         lsvd_status* st) {
+    const uint64_t key = hash_ns(count, n) ^ (uint64_t(prec) << 61);
+    auto it = ctx->plans.find(key);
+    if (it != ctx->plans.end() && it->second->count == count &&
+        std::equal(it->second->ns.begin(), it->second->ns.end(), n)) {
+        *st = LSVD_OK;
+        return it->second.get();
+    }
+    auto P = std::make_unique<BatchPlan>();
+    ClassShape shapes[kMaxClasses];
+    lsvd_autotune_shapes(ctx, prec, shapes);
+    *st = build_plan(ctx, count, n, shapes, *P);
+    if (*st != LSVD_OK) return nullptr;
+    if (ctx->plans.size() > 16) ctx->plans.clear();
+    BatchPlan* raw = P.get();
+    ctx->plans[key] = std::move(P);
+    return raw;
+}
+
+extern "C" lsvd_status lsvd_svd_batched_f64(lsvd_context* ctx, int64_t count, const int32_t* n,
+                                            const double* A, double* U, double* S, double* Vt,
+                                            lsvd_diag* diags, lsvd_precision precision,
+                                            uint32_t flags) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    if (count < 0 || (count > 0 && (!n || !A || !U || !S || !Vt)))
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_svd_batched_f64: bad pointer");
+    if (count == 0) return LSVD_OK;
+    if (count > (int64_t(1) << 30)) return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "batch too large");
+    for (int64_t t = 0; t < count; ++t)
+        if (n[t] < 1 || n[t] > kMaxN)
+            return lsvd_ctx_fail(ctx, n[t] < 1 ? LSVD_BAD_SHAPE : LSVD_UNSUPPORTED,
+                                 "lsvd_svd_batched_f64: every n must be in 1..64");
+    if (precision != LSVD_PREC_FP64 && precision != LSVD_PREC_MIXED_TF32 &&
+        precision != LSVD_PREC_MIXED_BF16)
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "unknown precision");
+    cudaSetDevice(ctx->device);
+    lsvd_status st;
+    BatchPlan* P = lsvd_get_plan(ctx, count, n, precision, &st);
+    if (!P) return st;
+    const bool dev = is_dev(flags);
+    const bool want_diag = (flags & LSVD_WANT_DIAG) != 0;
+    cudaError_t e;
+    const double* dA = A;
+    double *dU = U, *dS = S, *dV = Vt;
+    lsvd_diag* dD = diags;
+    if (!dev) {
+        dA = static_cast<double*>(P->d_a.get(size_t(P->a_elems) * 8, &e));
+        if (e == cudaSuccess) dU = static_cast<double*>(P->d_u.get(size_t(P->a_elems) * 8, &e));
+        if (e == cudaSuccess) dS = static_cast<double*>(P->d_s.get(size_t(P->s_elems) * 8, &e));
+        if (e == cudaSuccess) dV = static_cast<double*>(P->d_vt.get(size_t(P->a_elems) * 8, &e));
+        if (e == cudaSuccess && diags)
+            dD = static_cast<lsvd_diag*>(P->d_diag.get(size_t(count) * sizeof(lsvd_diag), &e));
+        if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "batch buffers");
+        if ((e = cudaMemcpyAsync(const_cast<double*>(dA), A, size_t(P->a_elems) * 8,
+                                 cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "copy A");
+    }
+    if ((st = lsvd_run_plan(ctx, *P, dA, dU, dS, dV, dD, want_diag, true)) != LSVD_OK) return st;
+    if (!dev) {
+        cudaStream_t s = ctx->stream;
+        if ((e = cudaMemcpyAsync(U, dU, size_t(P->a_elems) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(S, dS, size_t(P->s_elems) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(Vt, dV, size_t(P->a_elems) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (diags && (e = cudaMemcpyAsync(diags, dD, size_t(count) * sizeof(lsvd_diag),
+                                           cudaMemcpyDeviceToHost, s)) != cudaSuccess))
+            return lsvd_ctx_cuda(ctx, e, "copy out");
+    }
+    if (dev && (flags & LSVD_ASYNC)) return LSVD_OK;
+    int agg = 0;
+    if ((e = cudaMemcpyAsync(&agg, P->s_agg, 4, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "sync");
+    if (agg & LSVD_MAT_NONFINITE) return LSVD_NONFINITE_INPUT;
+    if (agg & LSVD_MAT_JACOBI_CAP) return LSVD_NOT_CONVERGED;
+    return LSVD_OK;
+}

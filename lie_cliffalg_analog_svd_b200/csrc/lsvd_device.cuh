@@ -1,0 +1,772 @@
+// lsvd_device.cuh -- device-side building blocks of the B200 SVD hot path.
+//
+// A "team" is 1, 2, 4 or 8 warps of a 256-thread CTA that solves one matrix
+// with everything resident in shared memory (n <= 64: three n x n FP64
+// buffers, column-major, leading dimension np+1 with np = n rounded up to 4,
+// which makes column walks and the interleaved GEMM tiles bank-conflict free).
+// Teams synchronise on their own named barrier (bar.sync id, 32*W), so up to
+// eight matrices progress independently inside one CTA.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "lsvd.h"
+
+namespace lsvd {
+
+constexpr int kMaxN = 64;
+constexpr int kCtaThreads = 256;
+
+struct Team {
+    int tid;       // 0 .. nthreads-1
+    int nthreads;  // 32 * nwarps
+    int warp;      // warp index inside the team
+    int lane;
+    int nwarps;
+    int bar;       // named barrier id (1..15)
+    __device__ __forceinline__ void sync() const {
+        if (nwarps == 1)
+            __syncwarp();
+        else
+            asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthreads) : "memory");
+    }
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum over aligned groups of G lanes (all 32 lanes must call).
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Deterministic team-wide sum (same value on every thread).  red >= nwarps.
+__device__ __forceinline__ double team_sum(const Team& t, double v, double* red) {
+    v = warp_sum(v);
+    if (t.nwarps == 1) return v;
+    if (t.lane == 0) red[t.warp] = v;
+    t.sync();
+    double s = 0.0;
+    for (int w = 0; w < t.nwarps; ++w) s += red[w];
+    t.sync();
+    return s;
+}
+
+__device__ __forceinline__ double team_max(const Team& t, double v, double* red) {
+    v = warp_max(v);
+    if (t.nwarps == 1) return v;
+    if (t.lane == 0) red[t.warp] = v;
+    t.sync();
+    double s = 0.0;
+    for (int w = 0; w < t.nwarps; ++w) s = fmax(s, red[w]);
+    t.sync();
+    return s;
+}
+
+// Register-tiled FP64 GEMM over a team: C(i, j) = sum_{k<kdim} a(k, i) b(k, j)
+// for i, j < np.  Each thread owns TS x TS outputs at rows ti + r*nt and
+// columns tj + c*nt (interleaved tiles, nt = np/TS): consecutive lanes touch
+// consecutive rows, so column-major operands stream conflict-free.
+// epi(i, j, value) consumes each output.
+template <int TS, class LA, class LB, class Epi>
+__device__ __forceinline__ void team_gemm(const Team& t, int np, int kdim, LA la, LB lb, Epi epi) {
+    const int nt = np / TS;
+    const int ntiles = nt * nt;
+    for (int tile = t.tid; tile < ntiles; tile += t.nthreads) {
+        const int ti = tile % nt, tj = tile / nt;
+        double acc[TS][TS];
+#pragma unroll
+        for (int r = 0; r < TS; ++r)
+#pragma unroll
+            for (int c = 0; c < TS; ++c) acc[r][c] = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < kdim; ++k) {
+            double av[TS], bv[TS];
+#pragma unroll
+            for (int r = 0; r < TS; ++r) av[r] = la(k, ti + r * nt);
+#pragma unroll
+            for (int c = 0; c < TS; ++c) bv[c] = lb(k, tj + c * nt);
+#pragma unroll
+            for (int r = 0; r < TS; ++r)
+#pragma unroll
+                for (int c = 0; c < TS; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+        }
+#pragma unroll
+        for (int r = 0; r < TS; ++r)
+#pragma unroll
+            for (int c = 0; c < TS; ++c) epi(ti + r * nt, tj + c * nt, acc[r][c]);
+    }
+}
+
+// Pair k of round-robin layer `layer` over m (= n rounded up to even)
+// indices: the circle method of layer_pairs, src/lie_svd_joint.rs:524-539.
+__device__ __forceinline__ void rr_pair(int m, int layer, int k, int& a, int& b) {
+    const int ring = m - 1;
+    if (k == 0) {
+        a = m - 1;
+        b = layer % ring;
+    } else {
+        a = (layer + k) % ring;
+        b = (layer + ring - k) % ring;
+    }
+}
+
+// ---------------------------------------------------------------- Micro ----
+// LieSvdMicro::solve (src/lie_svd_micro.rs:21-214) for one matrix per thread,
+// everything in registers.  Returns false when the reference would escalate
+// to LieSvdSmall (off-diagonal > 1e-10 max(||A||_F, 1), :90-92).
+
+__device__ __forceinline__ double wrap_half_pi(double a) {
+    const double kPi = 3.141592653589793238462643383279502884;
+    while (a > 0.5 * kPi) a -= kPi;
+    while (a < -0.5 * kPi) a += kPi;
+    return a;
+}
+
+template <int N>
+__device__ __forceinline__ double micro_offdiag(const double (&w)[N][N]) {
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            if (i != j) s += w[i][j] * w[i][j];
+    return sqrt(s);
+}
+
+template <int N>
+__device__ __forceinline__ void micro_rot_rows(double (&w)[N][N], int i, int j, double s, double c) {
+#pragma unroll
+    for (int col = 0; col < N; ++col) {
+        const double ai = w[i][col], aj = w[j][col];
+        w[i][col] = c * ai - s * aj;
+        w[j][col] = s * ai + c * aj;
+    }
+}
+template <int N>
+__device__ __forceinline__ void micro_rot_cols(double (&w)[N][N], int i, int j, double s, double c) {
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+        const double ai = w[r][i], aj = w[r][j];
+        w[r][i] = c * ai - s * aj;
+        w[r][j] = s * ai + c * aj;
+    }
+}
+
+struct MicroOut {
+    int sweeps;
+    int rotations;
+    bool ok;
+    bool nonfinite;
+};
+
+// Fixed pair schedules of src/lie_svd_micro.rs:41-48.
+__device__ __forceinline__ void micro_pair(int n, int k, int& i, int& j) {
+    if (n == 2) {
+        i = 0; j = 1;
+    } else if (n == 3) {
+        const int pi[3] = {0, 0, 1}, pj[3] = {1, 2, 2};
+        i = pi[k]; j = pj[k];
+    } else {
+        const int pi[6] = {0, 2, 0, 1, 0, 1}, pj[6] = {1, 3, 2, 3, 3, 2};
+        i = pi[k]; j = pj[k];
+    }
+}
+
+template <int N>
+__device__ MicroOut micro_solve_regs(const double* __restrict__ A, int64_t lda, double* U,
+                                     int64_t ldu, double* S, double* Vt, int64_t ldvt) {
+    MicroOut out{0, 0, true, false};
+    double w[N][N], ub[N][N], vb[N][N];
+    double fro2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            w[i][j] = A[i * lda + j];
+            fro2 += w[i][j] * w[i][j];
+            ub[i][j] = vb[i][j] = (i == j) ? 1.0 : 0.0;
+            if (!isfinite(w[i][j])) out.nonfinite = true;
+        }
+    const double ref = fmax(sqrt(fro2), 1e-300);
+    const double tol = 1e-13 * fmax(ref, 1.0);  // MICRO_TOL, :15 and :65
+    const int max_sweeps = (N == 2) ? 1 : 24;
+    constexpr int NP = (N == 2) ? 1 : (N == 3 ? 3 : 6);
+    for (int sw = 0; sw < max_sweeps; ++sw) {
+        const double e = micro_offdiag<N>(w);
+        if (e <= tol || !isfinite(e)) break;
+        out.sweeps = sw + 1;
+        bool changed = false;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            int i, j;
+            micro_pair(N, k, i, j);
+            if (fabs(w[i][j]) + fabs(w[j][i]) <= tol) continue;
+            // local_pair_svd_angles, :128-139
+            const double sum = atan2(-(w[i][j] + w[j][i]), w[i][i] - w[j][j]);
+            const double diff = atan2(w[i][j] - w[j][i], w[i][i] + w[j][j]);
+            const double tl = wrap_half_pi(0.5 * (sum + diff));
+            const double tr = wrap_half_pi(0.5 * (sum - diff));
+            if (fabs(tl) + fabs(tr) <= 1e-18) continue;
+            double sl, cl, sr, cr;
+            sincos(tl, &sl, &cl);
+            sincos(tr, &sr, &cr);
+            micro_rot_rows<N>(w, i, j, sl, cl);
+            micro_rot_cols<N>(ub, i, j, sl, cl);
+            micro_rot_cols<N>(w, i, j, sr, cr);
+            micro_rot_cols<N>(vb, i, j, sr, cr);
+            changed = true;
+            out.rotations++;
+        }
+        if (!changed) break;
+    }
+    if (micro_offdiag<N>(w) > 1e-10 * fmax(ref, 1.0)) {
+        out.ok = false;
+        return out;
+    }
+    // extract_sorted_svd, :187-214: stable sort by |diag| descending.
+    int order[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) order[i] = i;
+#pragma unroll
+    for (int i = 1; i < N; ++i) {
+        // insertion sort (stable): move order[i] left past smaller |diag|
+        for (int k = i; k > 0; --k) {
+            const int a = order[k - 1], b = order[k];
+            double da = 0, db = 0;
+#pragma unroll
+            for (int q = 0; q < N; ++q) {
+                if (q == a) da = fabs(w[q][q]);
+                if (q == b) db = fabs(w[q][q]);
+            }
+            if (da < db) {
+                order[k - 1] = b;
+                order[k] = a;
+            }
+        }
+    }
+#pragma unroll
+    for (int dst = 0; dst < N; ++dst) {
+        const int src = order[dst];
+        double d = 0.0;
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+            if (q == src) d = w[q][q];
+        S[dst] = fabs(d);
+        const double sg = d < 0.0 ? -1.0 : 1.0;
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+            double uv = 0.0, vv = 0.0;
+#pragma unroll
+            for (int q = 0; q < N; ++q)
+                if (q == src) {
+                    uv = ub[r][q];
+                    vv = vb[r][q];
+                }
+            U[r * ldu + dst] = sg * uv;
+            Vt[dst * ldvt + r] = vv;
+        }
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------- Small ----
+
+struct TeamScratch {
+    double red[8];
+    double sig[kMaxN];
+    int perm[kMaxN];
+    int cnt[4];
+    int rotor_idx;
+    int pad_;
+};
+
+__host__ __device__ constexpr int pad4(int n) { return (n + 3) & ~3; }
+// Doubles of shared memory one team needs for an n x n solve.
+__host__ __device__ constexpr int team_smem_doubles(int n) {
+    return 3 * (pad4(n) + 1) * pad4(n) + int(sizeof(TeamScratch) / sizeof(double));
+}
+
+struct SmallJob {
+    int n;
+    const double* A;
+    int64_t lda;
+    double* U;
+    int64_t ldu;
+    double* S;
+    double* Vt;
+    int64_t ldvt;
+    lsvd_diag* diag;  // may be null
+    lsvd_rotor* rotors;
+    int64_t rotor_cap;
+    int64_t* rotor_count;  // device, may be null
+    int32_t* perm_out;     // may be null
+    bool want_diag;
+    int extra_flags;  // e.g. LSVD_MAT_MICRO_FALLBACK
+    int* agg;         // OR of outcome flags over a batch (may be null)
+};
+
+// Loads row-major A (global) into column-major smem buffer B (np x np,
+// zero-padded).  Returns sum of squares and counts non-finite entries.
+__device__ __forceinline__ void load_colmajor(const Team& t, const SmallJob& job, int np, int ld,
+                                              double* B, double& fro2, int& bad) {
+    const int n = job.n;
+    for (int idx = t.tid; idx < np * np; idx += t.nthreads) {
+        const int i = idx / np, j = idx - (idx / np) * np;
+        double v = 0.0;
+        if (i < n && j < n) {
+            v = job.A[i * job.lda + j];
+            fro2 += v * v;
+            if (!isfinite(v)) bad++;
+        }
+        B[j * ld + i] = v;
+    }
+}
+
+// Modified Gram-Schmidt of the n columns of B (in place) with the
+// rank-deficient fill of gram_schmidt_orthonormal, src/lie_svd_small.rs:82-144.
+// Executed by warp 0 of the team (lanes hold rows lane and lane+32).
+__device__ inline void warp_mgs(const Team& t, double* B, int n, int ld) {
+    if (t.warp != 0) return;
+    const int l0 = t.lane, l1 = t.lane + 32;
+    auto col = [&](int j, int row) -> double { return row < n ? B[j * ld + row] : 0.0; };
+    for (int j = 0; j < n; ++j) {
+        double v0 = col(j, l0), v1 = col(j, l1);
+        for (int k = 0; k < j; ++k) {
+            const double q0 = col(k, l0), q1 = col(k, l1);
+            const double d = warp_sum(q0 * v0 + q1 * v1);
+            v0 -= d * q0;
+            v1 -= d * q1;
+        }
+        const double nrm = sqrt(warp_sum(v0 * v0 + v1 * v1));
+        if (nrm >= 1e-10) {
+            v0 /= nrm;
+            v1 /= nrm;
+        } else {
+            double best_norm = -1.0, b0 = 0.0, b1 = 0.0;
+            for (int kk = 0; kk < n; ++kk) {
+                double c0 = (l0 == kk) ? 1.0 : 0.0, c1 = (l1 == kk) ? 1.0 : 0.0;
+                for (int cc = 0; cc < j; ++cc) {
+                    const double q0 = col(cc, l0), q1 = col(cc, l1);
+                    const double d = warp_sum(q0 * c0 + q1 * c1);
+                    c0 -= d * q0;
+                    c1 -= d * q1;
+                }
+                const double en = sqrt(warp_sum(c0 * c0 + c1 * c1));
+                if (en > best_norm) {
+                    best_norm = en;
+                    b0 = c0;
+                    b1 = c1;
+                }
+            }
+            if (best_norm > 0.0 && isfinite(best_norm)) {
+                v0 = b0 / best_norm;
+                v1 = b1 / best_norm;
+            } else {
+                v0 = (l0 == j) ? 1.0 : 0.0;
+                v1 = (l1 == j) ? 1.0 : 0.0;
+            }
+        }
+        if (l0 < n) B[j * ld + l0] = v0;
+        if (l1 < n) B[j * ld + l1] = v1;
+        __syncwarp();
+    }
+}
+
+// One round-robin layer of one-sided (Hestenes) Jacobi on the columns of W,
+// accumulating V.  Each pair is handled by an aligned group of G lanes
+// (rows gl + G*r); the three Gram entries are group-shuffle reductions.
+template <int G>
+__device__ __forceinline__ void jacobi_layer(const Team& t, int n, int m, int layer, double* W,
+                                             double* V, int ld, double tol, TeamScratch* sc,
+                                             int cnt_slot, const SmallJob& job, uint32_t round) {
+    constexpr int R = kMaxN / G;
+    constexpr int GPW = 32 / G;
+    const int half = m >> 1;
+    const int gl = t.lane % G;
+    const int ngroups = t.nwarps * GPW;
+    for (int base = t.warp * GPW; base < half; base += ngroups) {
+        const int k = base + t.lane / G;
+        int a = 0, b = 0;
+        bool valid = k < half;
+        if (valid) {
+            rr_pair(m, layer, k, a, b);
+            valid = a < n && b < n;
+        }
+        const int p = min(a, b), q = max(a, b);
+        double wp[R], wq[R];
+        double al = 0.0, be = 0.0, ga = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int row = gl + G * r;
+            const bool in = valid && row < n;
+            wp[r] = in ? W[p * ld + row] : 0.0;
+            wq[r] = in ? W[q * ld + row] : 0.0;
+            al = fma(wp[r], wp[r], al);
+            be = fma(wq[r], wq[r], be);
+            ga = fma(wp[r], wq[r], ga);
+        }
+        al = group_sum<G>(al);
+        be = group_sum<G>(be);
+        ga = group_sum<G>(ga);
+        const bool rot = valid && ga != 0.0 && al > 0.0 && be > 0.0 &&
+                         fabs(ga) > tol * (sqrt(al) * sqrt(be));
+        if (rot) {
+            // Rutishauser tangent, as in eigh_jacobi_full (src/lie_svd_small.rs:235-242),
+            // applied to the 2x2 Gram block [[al, ga], [ga, be]].
+            const double th = (be - al) / (2.0 * ga);
+            const double tt = th >= 0.0 ? 1.0 / (th + sqrt(th * th + 1.0))
+                                        : -1.0 / (-th + sqrt(th * th + 1.0));
+            const double c = 1.0 / sqrt(tt * tt + 1.0);
+            const double s = tt * c;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int row = gl + G * r;
+                if (row < n) {
+                    W[p * ld + row] = c * wp[r] - s * wq[r];
+                    W[q * ld + row] = s * wp[r] + c * wq[r];
+                    const double vp = V[p * ld + row], vq = V[q * ld + row];
+                    V[p * ld + row] = c * vp - s * vq;
+                    V[q * ld + row] = s * vp + c * vq;
+                }
+            }
+            if (gl == 0) {
+                atomicAdd(&sc->cnt[cnt_slot], 1);
+                if (job.rotors) {
+                    const int idx = atomicAdd(&sc->rotor_idx, 1);
+                    if (idx < job.rotor_cap) {
+                        lsvd_rotor rr;
+                        rr.i = (uint16_t)p;
+                        rr.j = (uint16_t)q;
+                        rr.round = round;
+                        rr.theta = atan(tt);
+                        job.rotors[idx] = rr;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// LieSvdSmall::solve (src/lie_svd_small.rs:296-323) by one team, n <= 64.
+//   1. newton_schulz_polar (:158-183)  X <- 0.5 X (3I - X^T X), FP64 GEMMs in smem
+//   2. P = sym(Q^T A)                  (:305-309)
+//   3. eigensolve of P                 round-robin one-sided Jacobi (numerically
+//      equivalent to the reference's cyclic two-sided sweep on symmetric PSD P)
+//   4. U = Q V, orthogonality check, repair_left_basis_from_right (:185-208, :317-320)
+template <int TS, int G>
+__device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm) {
+    const int n = job.n;
+    const int np = pad4(n);
+    const int ld = np + 1;
+    double* X = sm;
+    double* T = X + ld * np;
+    double* Xn = T + ld * np;
+    TeamScratch* sc = reinterpret_cast<TeamScratch*>(Xn + ld * np);
+    const double refn = sqrt(double(n));
+    int flags = job.extra_flags;
+
+    // ---- load A, Frobenius norm, finiteness
+    double fro2 = 0.0;
+    int bad = 0;
+    load_colmajor(t, job, np, ld, X, fro2, bad);
+    fro2 = team_sum(t, fro2, sc->red);
+    const double nbad = team_sum(t, double(bad), sc->red);  // also syncs X
+    const double afro = sqrt(fro2);
+    if (nbad > 0.0) {
+        const double qnan = __longlong_as_double(0x7ff8000000000000ULL);
+        for (int idx = t.tid; idx < n * n; idx += t.nthreads) {
+            const int i = idx / n, j = idx % n;
+            job.U[i * job.ldu + j] = qnan;
+            job.Vt[i * job.ldvt + j] = qnan;
+        }
+        for (int i = t.tid; i < n; i += t.nthreads) {
+            job.S[i] = qnan;
+            if (job.perm_out) job.perm_out[i] = i;
+        }
+        if (t.tid == 0) {
+            if (job.diag) {
+                lsvd_diag d;
+                d.rel_recon = d.orth_u = d.orth_v = qnan;
+                d.ns_iters = 0;
+                d.jacobi_sweeps = 0;
+                d.rotations = 0;
+                d.flags = flags | LSVD_MAT_NONFINITE;
+                d.route = LSVD_ROUTE_SMALL;
+                *job.diag = d;
+            }
+            if (job.agg) atomicOr(job.agg, flags | LSVD_MAT_NONFINITE);
+            if (job.rotor_count) *job.rotor_count = 0;
+        }
+        t.sync();
+        return;
+    }
+
+    // ---- 1. Newton-Schulz polar
+    const double scale = fmax(afro, 1e-300);
+    for (int idx = t.tid; idx < n * n; idx += t.nthreads) {
+        const int i = idx % n, j = idx / n;
+        X[j * ld + i] = X[j * ld + i] / scale;
+    }
+    t.sync();
+    bool conv = false, diverged = false;
+    int iters = 0;
+    for (;;) {
+        team_gemm<TS>(
+            t, np, n, [&](int k, int i) { return X[i * ld + k]; },
+            [&](int k, int j) { return X[j * ld + k]; },
+            [&](int i, int j, double v) { T[j * ld + i] = v; });
+        t.sync();
+        if (conv || iters == 120) break;  // POLAR_MAX_ITERS, :67
+        iters++;
+        double d2 = 0.0;
+        team_gemm<TS>(
+            t, np, n, [&](int k, int i) { return X[k * ld + i]; },
+            [&](int k, int j) { return T[j * ld + k]; },
+            [&](int i, int j, double v) {
+                const double x = X[j * ld + i];
+                const double xn = 0.5 * (3.0 * x - v);
+                Xn[j * ld + i] = xn;
+                d2 += (xn - x) * (xn - x);
+            });
+        d2 = team_sum(t, d2, sc->red);
+        const double delta = sqrt(d2);
+        if (!isfinite(d2) || delta > 1e6 * refn) {
+            diverged = true;
+            break;
+        }
+        double* tmp = X;
+        X = Xn;
+        Xn = tmp;
+        if (delta < 1e-13 * refn) conv = true;  // POLAR_TOL, :68
+    }
+    bool polar_ok;
+    if (!diverged) {
+        double o2 = 0.0;
+        for (int idx = t.tid; idx < n * n; idx += t.nthreads) {
+            const int i = idx % n, j = idx / n;
+            const double d = T[j * ld + i] - (i == j ? 1.0 : 0.0);
+            o2 += d * d;
+        }
+        o2 = team_sum(t, o2, sc->red);
+        polar_ok = sqrt(o2) <= 1e-8 * refn;
+        if (!conv) flags |= LSVD_MAT_NS_CAP;
+    } else {
+        // (gram_schmidt_orthonormal(a), false), :169-171
+        polar_ok = false;
+        flags |= LSVD_MAT_NS_DIVERGED;
+        double f = 0.0;
+        int b2 = 0;
+        load_colmajor(t, job, np, ld, X, f, b2);
+        t.sync();
+        warp_mgs(t, X, n, ld);
+        t.sync();
+    }
+    if (!polar_ok) flags |= LSVD_MAT_POLAR_UNTRUSTED;
+    double* Q = X;
+    double* Wb = T;
+    double* Vb = Xn;
+
+    // ---- 2. P = sym(Q^T A)
+    {
+        double f = 0.0;
+        int b2 = 0;
+        load_colmajor(t, job, np, ld, Vb, f, b2);
+    }
+    t.sync();
+    team_gemm<TS>(
+        t, np, n, [&](int k, int i) { return Q[i * ld + k]; },
+        [&](int k, int j) { return Vb[j * ld + k]; },
+        [&](int i, int j, double v) { Wb[j * ld + i] = v; });
+    t.sync();
+    double amax = 0.0;
+    for (int idx = t.tid; idx < n * n; idx += t.nthreads) {
+        const int i = idx % n, j = idx / n;
+        if (i < j) {
+            const double s = (Wb[j * ld + i] + Wb[i * ld + j]) * 0.5;
+            Wb[j * ld + i] = s;
+            Wb[i * ld + j] = s;
+            amax = fmax(amax, fabs(s));
+        } else if (i == j) {
+            amax = fmax(amax, fabs(Wb[j * ld + i]));
+        }
+    }
+    amax = team_max(t, amax, sc->red);
+    // Power-of-two column scaling keeps the squared Gram entries of the
+    // one-sided sweep inside the f64 range (exact, undone on sigma).
+    const double wscale = amax > 0.0 ? ldexp(1.0, -ilogb(amax)) : 1.0;
+    for (int idx = t.tid; idx < np * np; idx += t.nthreads) {
+        const int i = idx % np, j = idx / np;
+        Wb[j * ld + i] = (i < n && j < n) ? Wb[j * ld + i] * wscale : 0.0;
+        Vb[j * ld + i] = (i == j && i < n) ? 1.0 : 0.0;
+    }
+    if (t.tid < 4) sc->cnt[t.tid] = 0;
+    if (t.tid == 0) sc->rotor_idx = 0;
+    t.sync();
+
+    // ---- 3. round-robin one-sided Jacobi on P
+    const int m = (n % 2 == 0) ? n : n + 1;
+    const int layers = (n % 2 == 0) ? (n > 0 ? n - 1 : 0) : n;  // round_robin_layer_count
+    const int max_sweeps = 60 + 20 * n;                           // eigh_jacobi_full, :216
+    const double jtol = sqrt(double(n)) * 2.220446049250313e-16;
+    int sweeps = 0;
+    long long rotations = 0;
+    for (int sw = 0; sw < max_sweeps; ++sw) {
+        const int slot = sw & 3;
+        if (t.tid == 0) sc->cnt[(sw + 2) & 3] = 0;
+        sweeps = sw + 1;
+        for (int layer = 0; layer < layers; ++layer) {
+            jacobi_layer<G>(t, n, m, layer, Wb, Vb, ld, jtol, sc, slot, job,
+                            uint32_t(sw * layers + layer));
+            t.sync();
+        }
+        const int rotated = sc->cnt[slot];
+        rotations += rotated;
+        if (rotated == 0) break;
+        if (sw + 1 == max_sweeps) flags |= LSVD_MAT_JACOBI_CAP;
+    }
+
+    // ---- sigma = column norms, descending stable sort
+    {
+        const int gpw = 32 / G;
+        for (int base = t.warp * gpw; base < n; base += t.nwarps * gpw) {
+            const int j = base + t.lane / G;
+            double s = 0.0;
+            for (int row = t.lane % G; row < n; row += G) {
+                const double w = j < n ? Wb[j * ld + row] : 0.0;
+                s = fma(w, w, s);
+            }
+            s = group_sum<G>(s);
+            if (j < n && t.lane % G == 0) sc->sig[j] = sqrt(s) / wscale;
+        }
+    }
+    t.sync();
+    for (int j = t.tid; j < n; j += t.nthreads) {
+        const double sj = sc->sig[j];
+        const double kj = isnan(sj) ? -1.0 : sj;
+        int rank = 0;
+        for (int k = 0; k < n; ++k) {
+            const double sk = sc->sig[k];
+            const double kk = isnan(sk) ? -1.0 : sk;
+            rank += (kk > kj) || (kk == kj && k < j);
+        }
+        sc->perm[rank] = j;
+    }
+    t.sync();
+    const int* perm = sc->perm;
+
+    // ---- 4. U = Q V (sorted); orthogonality check (:317-318)
+    double* Ub = Wb;  // W is no longer needed
+    team_gemm<TS>(
+        t, np, n, [&](int k, int i) { return Q[k * ld + i]; },
+        [&](int k, int j) { return j < n ? Vb[perm[j] * ld + k] : 0.0; },
+        [&](int i, int j, double v) { Ub[j * ld + i] = v; });
+    t.sync();
+    auto orth_of = [&](const double* B) -> double {
+        double o2 = 0.0;
+        team_gemm<TS>(
+            t, np, n,
+            [&](int k, int i) { return B[i * ld + k]; },
+            [&](int k, int j) { return B[j * ld + k]; },
+            [&](int i, int j, double v) {
+                if (i < n && j < n) {
+                    const double d = v - (i == j ? 1.0 : 0.0);
+                    o2 += d * d;
+                }
+            });
+        return sqrt(team_sum(t, o2, sc->red));
+    };
+    double orth_u = orth_of(Ub);
+    bool a_in_x = false;
+    if (!polar_ok || orth_u > 1e-8 * refn) {
+        // repair_left_basis_from_right, :185-208 (Q is dead: reuse its buffer for A)
+        flags |= LSVD_MAT_REPAIRED;
+        double f = 0.0;
+        int b2 = 0;
+        load_colmajor(t, job, np, ld, Q, f, b2);
+        a_in_x = true;
+        double smax = 0.0;
+        for (int k = 0; k < n; ++k) smax = fmax(smax, sc->sig[k]);
+        const double stol = 1e-12 * fmax(smax, 1.0);
+        t.sync();
+        team_gemm<TS>(
+            t, np, n, [&](int k, int i) { return Q[k * ld + i]; },
+            [&](int k, int j) { return j < n ? Vb[perm[j] * ld + k] : 0.0; },
+            [&](int i, int j, double v) {
+                const double sj = j < n ? sc->sig[perm[j]] : 0.0;
+                Ub[j * ld + i] = (j < n && sj > stol) ? v / sj : 0.0;
+            });
+        t.sync();
+        warp_mgs(t, Ub, n, ld);
+        t.sync();
+        if (job.want_diag) orth_u = orth_of(Ub);
+    }
+
+    // ---- outputs (row-major)
+    for (int idx = t.tid; idx < n * n; idx += t.nthreads) {
+        const int i = idx / n, j = idx % n;
+        job.U[i * job.ldu + j] = Ub[j * ld + i];
+        job.Vt[i * job.ldvt + j] = Vb[perm[i] * ld + j];
+    }
+    for (int i = t.tid; i < n; i += t.nthreads) {
+        job.S[i] = sc->sig[perm[i]];
+        if (job.perm_out) job.perm_out[i] = perm[i];
+    }
+
+    double rel_recon = __longlong_as_double(0x7ff8000000000000ULL), orth_v = rel_recon;
+    if (job.want_diag) {
+        orth_v = orth_of(Vb);
+        if (!a_in_x) {
+            double f = 0.0;
+            int b2 = 0;
+            load_colmajor(t, job, np, ld, Q, f, b2);
+            t.sync();
+        }
+        // metrics::compute rel_recon (src/lib.rs:157-159): ||U S V^T - A||_F / ||A||_F
+        double r2 = 0.0;
+        team_gemm<TS>(
+            t, np, n, [&](int k, int i) { return Ub[k * ld + i]; },
+            [&](int k, int j) { return j < n ? sc->sig[perm[k]] * Vb[perm[k] * ld + j] : 0.0; },
+            [&](int i, int j, double v) {
+                if (i < n && j < n) {
+                    const double d = v - Q[j * ld + i];
+                    r2 += d * d;
+                }
+            });
+        rel_recon = sqrt(team_sum(t, r2, sc->red)) / fmax(afro, 1e-300);
+    }
+    if (t.tid == 0) {
+        int nrot = sc->rotor_idx;
+        if (job.rotors && nrot > job.rotor_cap) flags |= LSVD_MAT_ROTOR_OVERFLOW;
+        if (job.rotor_count) *job.rotor_count = nrot;
+        if (job.agg && flags) atomicOr(job.agg, flags);
+        if (job.diag) {
+            lsvd_diag d;
+            d.rel_recon = rel_recon;
+            d.orth_u = job.want_diag ? orth_u : __longlong_as_double(0x7ff8000000000000ULL);
+            d.orth_v = orth_v;
+            d.ns_iters = iters;
+            d.jacobi_sweeps = sweeps;
+            d.rotations = rotations;
+            d.flags = flags;
+            d.route = LSVD_ROUTE_SMALL;
+            *job.diag = d;
+        }
+    }
+    t.sync();
+}
+
+}  // namespace lsvd
