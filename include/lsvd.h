@@ -160,6 +160,27 @@ LSVD_API lsvd_status lsvd_metrics_f64(lsvd_context* ctx, int64_t m, int64_t d, i
                                       const double* Vt, const double* sigma_ref, double* out,
                                       uint32_t flags);
 
+/* ----------------------------------------------------- rotor schedule ---- */
+/* target: 0 = "mzi_mesh", 1 = "fpga_rotor_mesh" (HardwareTarget,
+ * src/lie_svd_compiler.rs:12-25).  The JSON text (NUL-terminated) is written
+ * to json[0..cap); *len receives its length without the NUL.  A too-small
+ * buffer returns LSVD_ROTOR_OVERFLOW with *len set (pass json=NULL to size).
+ * Host-side serialisation; no GPU is needed. */
+
+/* Replaces HardwareSchedule::from_orthogonal_matrix + to_json_string
+ * (src/lie_svd_compiler.rs:144-198, :213-265).  V d*d row-major. */
+LSVD_API lsvd_status lsvd_schedule_from_orthogonal(int64_t d, const double* V, int32_t target,
+                                                   char* json, int64_t cap, int64_t* len);
+
+/* phase-schedule-v1 schedule of a rotor stream (lsvd_small_solve_f64's
+ * `rotors`): one event per accepted rotation, layer = round, in the
+ * compiler's reconstruction convention (src/lie_svd_compiler.rs:396-411),
+ * source "gpu_jacobi", kind "jacobi_rotation".  It reconstructs the
+ * eigenbasis before the descending sort; the solver's `perm` orders it. */
+LSVD_API lsvd_status lsvd_schedule_from_rotors(const lsvd_rotor* rotors, int64_t count,
+                                               int64_t channels, int32_t target, char* json,
+                                               int64_t cap, int64_t* len);
+
 #ifdef __cplusplus
 }
 #endif

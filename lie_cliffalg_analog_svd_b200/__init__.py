@@ -7,8 +7,9 @@ API over that ABI.  Importing the package does not load the library;
 the first call does, and fails loudly if it was not built.
 """
 from .api import (Context, LieSvd, LieSvdMicro, LieSvdSmall, SmallResult, SvdMetrics,  # noqa: F401
-                  default_context, metrics, packed_offsets, svd_batched, unpack)
+                  HardwareSchedule, default_context, metrics, packed_offsets, svd_batched,
+                  unpack)
 from ._lib import LsvdError  # noqa: F401
 
-__all__ = ["Context", "LieSvd", "LieSvdMicro", "LieSvdSmall", "SmallResult", "SvdMetrics",
+__all__ = ["Context", "HardwareSchedule", "LieSvd", "LieSvdMicro", "LieSvdSmall", "SmallResult", "SvdMetrics",
            "default_context", "metrics", "packed_offsets", "svd_batched", "unpack", "LsvdError"]

@@ -293,3 +293,39 @@ def unpack(ns, packed, square: bool = True):
         blk = packed[off[t]:off[t + 1]]
         out.append(blk.reshape(n, n) if square else blk)
     return out
+
+
+TARGETS = {"mzi_mesh": 0, "fpga_rotor_mesh": 1}
+
+
+def _json_call(fn, *args) -> str:
+    n = C.c_int64(0)
+    st = fn(*args, None, 0, C.byref(n))
+    if st not in (L.OK,):
+        raise L.LsvdError(st, "schedule sizing failed")
+    buf = C.create_string_buffer(n.value + 1)
+    st = fn(*args, buf, n.value + 1, C.byref(n))
+    if st != L.OK:
+        raise L.LsvdError(st, "schedule serialisation failed")
+    return buf.value.decode()
+
+
+class HardwareSchedule:
+    """``HardwareSchedule`` (src/lie_svd_compiler.rs:43-266) as produced by the
+    library's host-side compiler; ``to_json_string`` is the library's JSON."""
+
+    @staticmethod
+    def from_orthogonal_matrix_json(v, target: str = "mzi_mesh") -> str:
+        v = _f64(v)
+        d = v.shape[0]
+        if v.ndim != 2 or v.shape[1] != d:
+            raise L.LsvdError(L.BAD_SHAPE, "HardwareSchedule::from_orthogonal_matrix: matrix must be square")
+        lib = L.load()
+        return _json_call(lib.lsvd_schedule_from_orthogonal, d, _ptr(v), TARGETS[target])
+
+    @staticmethod
+    def from_rotor_stream_json(rotors, channels: int, target: str = "mzi_mesh") -> str:
+        r = np.ascontiguousarray(rotors, dtype=L.ROTOR_DTYPE)
+        lib = L.load()
+        return _json_call(lib.lsvd_schedule_from_rotors, _ptr(r) if r.size else None, r.size,
+                          channels, TARGETS[target])

@@ -57,7 +57,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     Returns the library path."""
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _deps_mtime():
         return LIB
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []

@@ -173,7 +173,7 @@ lsvd_status lsvd_single_small(lsvd_context* ctx, int64_t n, const double* A, int
                               double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
                               lsvd_diag* diag, lsvd_rotor* rotors, int64_t rotor_cap,
                               int64_t* rotor_count, int32_t* perm, uint32_t flags,
-                              int extra_flags) {
+                              int extra_flags, bool host_meta) {
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (n < 1 || n > kMaxN)
         return lsvd_ctx_fail(ctx, n < 1 ? LSVD_BAD_SHAPE : LSVD_UNSUPPORTED,
@@ -242,17 +242,18 @@ lsvd_status lsvd_single_small(lsvd_context* ctx, int64_t n, const double* A, int
             return lsvd_ctx_cuda(ctx, e, "copy rotors");
     }
     if (rotor_count) {
-        if (dev)
-            cudaMemcpy(rotor_count, &hcount, 8, cudaMemcpyHostToDevice);
+        if (dev && !host_meta)
+            e = cudaMemcpy(rotor_count, &hcount, 8, cudaMemcpyHostToDevice);
         else
             *rotor_count = hcount;
     }
     if (diag) {
-        if (dev)
-            cudaMemcpy(diag, &hdiag, sizeof(hdiag), cudaMemcpyHostToDevice);
+        if (dev && !host_meta)
+            e = cudaMemcpy(diag, &hdiag, sizeof(hdiag), cudaMemcpyHostToDevice);
         else
             *diag = hdiag;
     }
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "copy diag out");
     if (hdiag.flags & LSVD_MAT_NONFINITE) return LSVD_NONFINITE_INPUT;
     if (hdiag.flags & LSVD_MAT_JACOBI_CAP) return LSVD_NOT_CONVERGED;
     if (rotors && hcount > rotor_cap) return LSVD_ROTOR_OVERFLOW;
@@ -265,7 +266,7 @@ extern "C" lsvd_status lsvd_small_solve_f64(lsvd_context* ctx, int64_t n, const 
                                             lsvd_rotor* rotors, int64_t rotor_cap,
                                             int64_t* rotor_count, int32_t* perm, uint32_t flags) {
     return lsvd_single_small(ctx, n, A, lda, U, ldu, S, Vt, ldvt, diag, rotors, rotor_cap,
-                             rotor_count, perm, flags, 0);
+                             rotor_count, perm, flags, 0, false);
 }
 
 extern "C" lsvd_status lsvd_micro_solve_f64(lsvd_context* ctx, int64_t n, const double* A,
@@ -301,7 +302,7 @@ extern "C" lsvd_status lsvd_micro_solve_f64(lsvd_context* ctx, int64_t n, const 
         return lsvd_ctx_cuda(ctx, e, "sync");
     if (hflag) {  // LieSvdMicro -> LieSvdSmall escalation, src/lie_svd_micro.rs:90-92
         return lsvd_single_small(ctx, n, A, lda, U, ldu, S, Vt, ldvt, diag, nullptr, 0, nullptr,
-                                 nullptr, flags, LSVD_MAT_MICRO_FALLBACK);
+                                 nullptr, flags, LSVD_MAT_MICRO_FALLBACK, false);
     }
     if ((e = copy2d(U, ldu, dU, n, n, n, st)) != cudaSuccess ||
         (e = copy2d(Vt, ldvt, dV, n, n, n, st)) != cudaSuccess ||
@@ -312,10 +313,12 @@ extern "C" lsvd_status lsvd_micro_solve_f64(lsvd_context* ctx, int64_t n, const 
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return lsvd_ctx_cuda(ctx, e, "sync");
     if (diag) {
-        if (is_dev(flags))
-            cudaMemcpy(diag, &hdiag, sizeof(hdiag), cudaMemcpyHostToDevice);
-        else
+        if (is_dev(flags)) {
+            if ((e = cudaMemcpy(diag, &hdiag, sizeof(hdiag), cudaMemcpyHostToDevice)) != cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "copy diag out");
+        } else {
             *diag = hdiag;
+        }
     }
     return (hdiag.flags & LSVD_MAT_NONFINITE) ? LSVD_NONFINITE_INPUT : LSVD_OK;
 }
@@ -368,8 +371,9 @@ static uint64_t hash_ns(int64_t count, const int32_t* n) {
 // Builds the LPT schedule: matrices sorted by n descending, grouped into work
 // items of one size class each.
 static lsvd_status build_plan(lsvd_context* ctx, int64_t count, const int32_t* n,
-                              const ClassShape* shapes, BatchPlan& P) {
+                              const ClassShape* shapes, lsvd_precision prec, BatchPlan& P) {
     P.count = count;
+    P.precision = prec;
     P.ns.assign(n, n + count);
     std::vector<int32_t> perm(static_cast<size_t>(count));
     std::iota(perm.begin(), perm.end(), 0);
@@ -393,7 +397,8 @@ static lsvd_status build_plan(lsvd_context* ctx, int64_t count, const int32_t* n
         cfg.variant = variant_of(s.ts, s.g);
         const int lo = c == 0 ? 1 : kClassHi[c - 1] + 1;
         const int hi = kClassHi[c];
-        cfg.slice = s.nwarps ? team_smem_doubles(hi) : 0;
+        cfg.slice = !s.nwarps ? 0 : (prec == LSVD_PREC_FP64 ? team_smem_doubles(hi)
+                                                             : mixed_smem_doubles(hi));
         if (lo > hi) continue;
     }
     size_t i = 0;
@@ -479,7 +484,12 @@ static cudaError_t enqueue_plan(lsvd_context* ctx, BatchPlan& P, const double* A
     if (e != cudaSuccess) return e;
     const int smem = std::max(P.smem_bytes, 16);
     const int grid = std::max(1, std::min(P.n_items, 2 * ctx->num_sms));
-    batched_kernel<<<grid, kCtaThreads, smem, st>>>(a);
+    if (P.precision == LSVD_PREC_MIXED_TF32)
+        batched_mixed_kernel<kPrecTF32><<<grid, kCtaThreads, smem, st>>>(a);
+    else if (P.precision == LSVD_PREC_MIXED_BF16)
+        batched_mixed_kernel<kPrecBF16><<<grid, kCtaThreads, smem, st>>>(a);
+    else
+        batched_kernel<<<grid, kCtaThreads, smem, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int fsmem = team_smem_doubles(4) * 8;
     fallback_kernel<<<std::max(1, std::min(ctx->num_sms, int(P.count))), kCtaThreads, fsmem, st>>>(a);
@@ -488,8 +498,15 @@ static cudaError_t enqueue_plan(lsvd_context* ctx, BatchPlan& P, const double* A
 
 lsvd_status lsvd_run_plan(lsvd_context* ctx, BatchPlan& P, const double* A, double* U, double* S,
                           double* Vt, lsvd_diag* diag, bool want_diag, bool use_graph) {
-    cudaError_t e = cudaFuncSetAttribute(batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         std::max(P.smem_bytes, 16));
+    const int sm_bytes = std::max(P.smem_bytes, 16);
+    cudaError_t e = P.precision == LSVD_PREC_MIXED_TF32
+                        ? cudaFuncSetAttribute(batched_mixed_kernel<kPrecTF32>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, sm_bytes)
+                    : P.precision == LSVD_PREC_MIXED_BF16
+                        ? cudaFuncSetAttribute(batched_mixed_kernel<kPrecBF16>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, sm_bytes)
+                        : cudaFuncSetAttribute(batched_kernel,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, sm_bytes);
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "smem attribute");
     if (!use_graph) {
         if ((e = enqueue_plan(ctx, P, A, U, S, Vt, diag, want_diag)) != cudaSuccess)
@@ -535,7 +552,7 @@ BatchPlan* lsvd_get_plan(lsvd_context* ctx, int64_t count, const int32_t* n, lsv
     auto P = std::make_unique<BatchPlan>();
     ClassShape shapes[kMaxClasses];
     lsvd_autotune_shapes(ctx, prec, shapes);
-    *st = build_plan(ctx, count, n, shapes, *P);
+    *st = build_plan(ctx, count, n, shapes, prec, *P);
     if (*st != LSVD_OK) return nullptr;
     if (ctx->plans.size() > 16) ctx->plans.clear();
     BatchPlan* raw = P.get();

@@ -38,8 +38,14 @@ static std::string cache_path() {
     return std::string(home ? home : "/tmp") + "/.cache/lsvd_b200/shapes.json";
 }
 
-void lsvd_autotune_shapes(lsvd_context* /*ctx*/, lsvd_precision /*prec*/, ClassShape* shapes) {
+void lsvd_autotune_shapes(lsvd_context* /*ctx*/, lsvd_precision prec, ClassShape* shapes) {
     for (int c = 0; c < lsvd::kMaxClasses; ++c) shapes[c] = lsvd_default_shape(c);
+    if (prec != LSVD_PREC_FP64) {
+        // the mixed path's FP32 tensor-core buffers are padded to 16: for
+        // n in 17..32 two teams of four warps keep two CTAs per SM
+        shapes[3] = ClassShape{4, 2, 8, 1};
+        shapes[4] = ClassShape{4, 4, 8, 1};
+    }
     // cache: a single line {"shapes": "cls:w,ts,g,pt;..."}
     if (FILE* f = std::fopen(cache_path().c_str(), "r")) {
         char buf[1024] = {0};

@@ -285,9 +285,13 @@ __device__ MicroOut micro_solve_regs(const double* __restrict__ A, int64_t lda, 
 
 // ---------------------------------------------------------------- Small ----
 
-struct TeamScratch {
+struct alignas(16) TeamScratch {
     double red[8];
     double sig[kMaxN];
+    // rotation of each pair of the current round-robin layer (two-sided sweep)
+    double rc[kMaxN / 2], rs[kMaxN / 2], rt[kMaxN / 2];
+    int rp[kMaxN / 2], rq[kMaxN / 2];
+    int pidx[2][kMaxN];  // index held at each position (ping-pong by layer parity)
     int perm[kMaxN];
     int cnt[4];
     int rotor_idx;
@@ -386,13 +390,28 @@ __device__ inline void warp_mgs(const Team& t, double* B, int n, int ld) {
     }
 }
 
-// One round-robin layer of one-sided (Hestenes) Jacobi on the columns of W,
-// accumulating V.  Each pair is handled by an aligned group of G lanes
-// (rows gl + G*r); the three Gram entries are group-shuffle reductions.
 template <int G>
-__device__ __forceinline__ void jacobi_layer(const Team& t, int n, int m, int layer, double* W,
-                                             double* V, int ld, double tol, TeamScratch* sc,
-                                             int cnt_slot, const SmallJob& job, uint32_t round) {
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+
+struct LayerStats {
+    int nrot;     // rotations recorded by this thread (group leaders only)
+    float cmax2;  // largest squared cosine this thread saw before rotating
+};
+
+// One round-robin layer of one-sided (Hestenes) Jacobi on the columns of W,
+// accumulating V, in precision Real (double, or float for the low-precision
+// phase of the mixed path).  Each pair is handled by an aligned group of G
+// lanes (rows gl + G*r); the three Gram entries are group-shuffle reductions.
+template <class Real, int G>
+__device__ __forceinline__ void jacobi_layer(const Team& t, int n, int m, int layer, Real* W,
+                                             Real* V, int ld, Real tol2, TeamScratch* sc,
+                                             const SmallJob& job, uint32_t round, LayerStats& st) {
     constexpr int R = kMaxN / G;
     constexpr int GPW = 32 / G;
     const int half = m >> 1;
@@ -407,14 +426,17 @@ __device__ __forceinline__ void jacobi_layer(const Team& t, int n, int m, int la
             valid = a < n && b < n;
         }
         const int p = min(a, b), q = max(a, b);
-        double wp[R], wq[R];
-        double al = 0.0, be = 0.0, ga = 0.0;
+        Real wp[R], wq[R], vp[R], vq[R];
+        Real al = 0, be = 0, ga = 0;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int row = gl + G * r;
             const bool in = valid && row < n;
-            wp[r] = in ? W[p * ld + row] : 0.0;
-            wq[r] = in ? W[q * ld + row] : 0.0;
+            wp[r] = in ? W[p * ld + row] : Real(0);
+            wq[r] = in ? W[q * ld + row] : Real(0);
+            // V is prefetched so its latency overlaps the reductions
+            vp[r] = in ? V[p * ld + row] : Real(0);
+            vq[r] = in ? V[q * ld + row] : Real(0);
             al = fma(wp[r], wp[r], al);
             be = fma(wq[r], wq[r], be);
             ga = fma(wp[r], wq[r], ga);
@@ -422,29 +444,34 @@ __device__ __forceinline__ void jacobi_layer(const Team& t, int n, int m, int la
         al = group_sum<G>(al);
         be = group_sum<G>(be);
         ga = group_sum<G>(ga);
-        const bool rot = valid && ga != 0.0 && al > 0.0 && be > 0.0 &&
-                         fabs(ga) > tol * (sqrt(al) * sqrt(be));
+        // Columns are scaled so that al, be <= 4n: the squared test cannot
+        // overflow, and it needs no square roots.
+        const Real ab = al * be;
+        const bool rot = valid && ga != Real(0) && al > Real(0) && be > Real(0) && ga * ga > tol2 * ab;
         if (rot) {
-            // Rutishauser tangent, as in eigh_jacobi_full (src/lie_svd_small.rs:235-242),
-            // applied to the 2x2 Gram block [[al, ga], [ga, be]].
-            const double th = (be - al) / (2.0 * ga);
-            const double tt = th >= 0.0 ? 1.0 / (th + sqrt(th * th + 1.0))
-                                        : -1.0 / (-th + sqrt(th * th + 1.0));
-            const double c = 1.0 / sqrt(tt * tt + 1.0);
-            const double s = tt * c;
+            st.cmax2 = fmaxf(st.cmax2, float((ga * ga) / ab));
+            // Rutishauser's smaller-root tangent of eigh_jacobi_full
+            // (src/lie_svd_small.rs:235-242) for the 2x2 Gram block
+            // [[al, ga], [ga, be]]: with zeta = (be - al) / (2 ga),
+            // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2))
+            //   = sign(be - al) * 2 ga / (|be - al| + hypot(be - al, 2 ga)).
+            const Real dd = be - al, g2 = Real(2) * ga;
+            const Real tt0 = g2 / (fabs(dd) + sqrt(fma(dd, dd, g2 * g2)));
+            const Real tt = dd < Real(0) ? -tt0 : tt0;
+            const Real c = rsqrt_t(fma(tt, tt, Real(1)));
+            const Real s = tt * c;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int row = gl + G * r;
                 if (row < n) {
                     W[p * ld + row] = c * wp[r] - s * wq[r];
                     W[q * ld + row] = s * wp[r] + c * wq[r];
-                    const double vp = V[p * ld + row], vq = V[q * ld + row];
-                    V[p * ld + row] = c * vp - s * vq;
-                    V[q * ld + row] = s * vp + c * vq;
+                    V[p * ld + row] = c * vp[r] - s * vq[r];
+                    V[q * ld + row] = s * vp[r] + c * vq[r];
                 }
             }
             if (gl == 0) {
-                atomicAdd(&sc->cnt[cnt_slot], 1);
+                st.nrot++;
                 if (job.rotors) {
                     const int idx = atomicAdd(&sc->rotor_idx, 1);
                     if (idx < job.rotor_cap) {
@@ -452,13 +479,207 @@ __device__ __forceinline__ void jacobi_layer(const Team& t, int n, int m, int la
                         rr.i = (uint16_t)p;
                         rr.j = (uint16_t)q;
                         rr.round = round;
-                        rr.theta = atan(tt);
+                        rr.theta = atan(double(tt));
                         job.rotors[idx] = rr;
                     }
                 }
             }
         }
     }
+}
+
+// Round-robin one-sided Jacobi sweeps on W (n columns) accumulating V until
+// a sweep rotates nothing, or the largest cosine a sweep met is <= stop_cos
+// (quadratic convergence: the next sweep would only see rounding noise), or
+// max_sweeps.  Rotates pairs whose cosine exceeds tol.  Returns sweeps run;
+// adds the rotation count to *rotations; sets *capped if max_sweeps was hit.
+template <class Real, int G>
+__device__ int jacobi_sweeps(const Team& t, int n, Real* W, Real* V, int ld, Real tol,
+                             float stop_cos, int max_sweeps, TeamScratch* sc, const SmallJob& job,
+                             long long* rotations, bool* capped) {
+    const int m = (n % 2 == 0) ? n : n + 1;
+    const int layers = (n % 2 == 0) ? (n > 0 ? n - 1 : 0) : n;  // round_robin_layer_count
+    const Real tol2 = tol * tol;
+    int sweeps = 0;
+    *capped = false;
+    for (int sw = 0; sw < max_sweeps; ++sw) {
+        sweeps = sw + 1;
+        LayerStats st{0, 0.0f};
+        for (int layer = 0; layer < layers; ++layer) {
+            jacobi_layer<Real, G>(t, n, m, layer, W, V, ld, tol2, sc, job,
+                                  uint32_t(sw * layers + layer), st);
+            t.sync();
+        }
+        const int rotated = int(team_sum(t, double(st.nrot), sc->red));
+        const double cmax2 = team_max(t, double(st.cmax2), sc->red);
+        *rotations += rotated;
+        if (rotated == 0 || cmax2 <= double(stop_cos) * double(stop_cos)) break;
+        if (sw + 1 == max_sweeps) *capped = true;
+    }
+    return sweeps;
+}
+
+// Position of index i in round-robin layer l over m indices (ring = m - 1):
+// pair k occupies positions 2k (smaller index) and 2k + 1 (larger index).
+__device__ __forceinline__ int rr_position(int m, int l, int i) {
+    const int ring = m - 1, half = m >> 1;
+    if (i == m - 1) return 1;  // always in pair 0 with l % ring, and the larger index
+    int d = i - l;  // 0 <= i, l < ring
+    if (d < 0) d += ring;
+    int k, j;
+    if (d == 0) {
+        k = 0;
+        j = m - 1;
+    } else if (d <= half - 1) {
+        k = d;
+        j = l + ring - k;
+        if (j >= ring) j -= ring;
+    } else {
+        k = ring - d;
+        j = l + k;
+        if (j >= ring) j -= ring;
+    }
+    return 2 * k + (i > j ? 1 : 0);
+}
+
+// Two-sided round-robin Jacobi of eigh_jacobi_full (src/lie_svd_small.rs:
+// 212-285) with P kept in pair-position order: in layer l, positions 2k and
+// 2k+1 hold the pair (p_k < q_k), so every 2x2 block R_a^T P[a,b] R_b is two
+// contiguous double2 loads, and the transformed block is written straight to
+// the next layer's positions in the other buffer (ping-pong B0/B1, leading
+// dimension m).  V stays in natural order.  Every warp computes the angles of
+// all pairs of the layer itself (lane k <-> pair k, m <= 64) and fetches them
+// by shuffle, so a layer costs one barrier.  Rotation: the reference's
+// smaller-root tangent (:235-242) written t = sign(d) 2 a_pq / (|d| +
+// hypot(d, 2 a_pq)), d = a_qq - a_pp; skip if |a_pq| < 1e-300; exact diagonal
+// update (:244-249).  Convergence test at sweep start: sqrt(sum_{p<q}
+// P_pq^2) < 1e-13 ||P||_F (:220-228).  On return *Pout holds P in the
+// positions of sc->pidx[*par]; returns the sweeps started.
+__device__ inline int jacobi2pp_sweeps(const Team& t, int n, double* B0, double* B1, double* V,
+                                       int ldv, double ref_norm, int max_sweeps, TeamScratch* sc,
+                                       const SmallJob& job, long long* rotations, bool* capped,
+                                       double** Pout, int* par) {
+    const int m = (n % 2 == 0) ? n : n + 1;
+    const int half = m >> 1;
+    const int layers = (n % 2 == 0) ? (n > 0 ? n - 1 : 0) : n;
+    int sweeps = 0;
+    *capped = false;
+    double* cur = B0;
+    double* nxt = B1;
+    int cp = 0;  // parity of sc->pidx describing cur
+    const int lane = t.lane;
+    for (int sw = 0; sw < max_sweeps; ++sw) {
+        sweeps = sw + 1;
+        double off = 0.0;
+        for (int idx = t.tid; idx < m * m; idx += t.nthreads) {
+            const int x = idx % m, y = idx / m;
+            if (x != y) off = fma(cur[y * m + x], cur[y * m + x], off);
+        }
+        off = 0.5 * team_sum(t, off, sc->red);
+        if (sqrt(off) < 1e-13 * ref_norm) break;  // JACOBI_TOL, :69
+        if (sw + 1 == max_sweeps) *capped = true;
+        int nrot = 0;
+        for (int l = 0; l < layers; ++l) {
+            const int lnext = (l + 1 == layers) ? 0 : l + 1;
+            // every warp: lane k computes the rotation of pair k
+            double c = 1.0, s = 0.0, tt = 0.0;
+            int xk = 0, yk = 0;
+            if (lane < half) {
+                const int k = lane;
+                const int p = sc->pidx[cp][2 * k], q = sc->pidx[cp][2 * k + 1];
+                if (q < n) {
+                    const double2 d0 = *reinterpret_cast<const double2*>(cur + (2 * k) * m + 2 * k);
+                    const double2 d1 = *reinterpret_cast<const double2*>(cur + (2 * k + 1) * m + 2 * k);
+                    const double apq = d1.x;
+                    if (fabs(apq) >= 1e-300) {
+                        const double dd = d1.y - d0.x, g2 = 2.0 * apq;
+                        const double t0 = g2 / (fabs(dd) + sqrt(fma(dd, dd, g2 * g2)));
+                        tt = dd < 0.0 ? -t0 : t0;
+                        c = rsqrt(fma(tt, tt, 1.0));
+                        s = tt * c;
+                    }
+                }
+                xk = rr_position(m, lnext, p);
+                yk = rr_position(m, lnext, q);
+                if (t.warp == 0) {
+                    sc->pidx[cp ^ 1][xk] = p;
+                    sc->pidx[cp ^ 1][yk] = q;
+                    if (s != 0.0) {
+                        nrot++;
+                        if (job.rotors) {
+                            const int ri = atomicAdd(&sc->rotor_idx, 1);
+                            if (ri < job.rotor_cap) {
+                                lsvd_rotor rr;
+                                rr.i = (uint16_t)p;
+                                rr.j = (uint16_t)q;
+                                rr.round = uint32_t(sw * layers + l);
+                                rr.theta = atan(tt);
+                                job.rotors[ri] = rr;
+                            }
+                        }
+                    }
+                }
+            }
+            // P <- J^T P J into the next layer's positions
+            const int nb = half * half;
+            for (int base = t.warp * 32; base < nb; base += t.nthreads) {
+                const int bi = base + lane;
+                const int a = bi % half, b = bi / half;
+                const double ca = __shfl_sync(0xffffffffu, c, a), sa = __shfl_sync(0xffffffffu, s, a);
+                const double cb = __shfl_sync(0xffffffffu, c, b & 31), sb = __shfl_sync(0xffffffffu, s, b & 31);
+                const double ta = __shfl_sync(0xffffffffu, tt, a);
+                const int xa = __shfl_sync(0xffffffffu, xk, a), ya = __shfl_sync(0xffffffffu, yk, a);
+                const int xb = __shfl_sync(0xffffffffu, xk, b & 31), yb = __shfl_sync(0xffffffffu, yk, b & 31);
+                if (bi >= nb) continue;
+                const double2 c0 = *reinterpret_cast<const double2*>(cur + (2 * b) * m + 2 * a);
+                const double2 c1 = *reinterpret_cast<const double2*>(cur + (2 * b + 1) * m + 2 * a);
+                if (a == b) {
+                    // c0 = (P_pp, P_qp), c1 = (P_pq, P_qq)
+                    double d00 = c0.x, d11 = c1.y, d01 = c1.x, d10 = c0.y;
+                    if (sa != 0.0) {
+                        d00 = c0.x - ta * c1.x;
+                        d11 = c1.y + ta * c1.x;
+                        d01 = 0.0;
+                        d10 = 0.0;
+                    }
+                    nxt[xa * m + xa] = d00;
+                    nxt[ya * m + ya] = d11;
+                    nxt[ya * m + xa] = d01;
+                    nxt[xa * m + ya] = d10;
+                    continue;
+                }
+                // block rows (p_a, q_a) x cols (p_b, q_b): b00 = c0.x, b10 = c0.y, b01 = c1.x, b11 = c1.y
+                const double x00 = cb * c0.x - sb * c1.x, x01 = sb * c0.x + cb * c1.x;
+                const double x10 = cb * c0.y - sb * c1.y, x11 = sb * c0.y + cb * c1.y;
+                nxt[xb * m + xa] = ca * x00 - sa * x10;
+                nxt[xb * m + ya] = sa * x00 + ca * x10;
+                nxt[yb * m + xa] = ca * x01 - sa * x11;
+                nxt[yb * m + ya] = sa * x01 + ca * x11;
+            }
+            // V <- V J (natural order); item = (pair b, row i)
+            const int nv = half * n;
+            for (int base = t.warp * 32; base < nv; base += t.nthreads) {
+                const int vi = base + lane;
+                const int b = vi / n, i = vi - (vi / n) * n;
+                const double cb = __shfl_sync(0xffffffffu, c, b & 31), sb = __shfl_sync(0xffffffffu, s, b & 31);
+                if (vi >= nv) continue;
+                const int ib = sc->pidx[cp][2 * b], jb = sc->pidx[cp][2 * b + 1];
+                if (jb >= n || sb == 0.0) continue;
+                const double vp = V[ib * ldv + i], vq = V[jb * ldv + i];
+                V[ib * ldv + i] = cb * vp - sb * vq;
+                V[jb * ldv + i] = sb * vp + cb * vq;
+            }
+            t.sync();
+            double* tmp = cur;
+            cur = nxt;
+            nxt = tmp;
+            cp ^= 1;
+        }
+        *rotations += (long long)team_sum(t, double(nrot), sc->red);
+    }
+    *Pout = cur;
+    *par = cp;
+    return sweeps;
 }
 
 // LieSvdSmall::solve (src/lie_svd_small.rs:296-323) by one team, n <= 64.
@@ -592,84 +813,82 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
         [&](int k, int j) { return Vb[j * ld + k]; },
         [&](int i, int j, double v) { Wb[j * ld + i] = v; });
     t.sync();
-    double amax = 0.0;
-    for (int idx = t.tid; idx < n * n; idx += t.nthreads) {
-        const int i = idx % n, j = idx / n;
-        if (i < j) {
-            const double s = (Wb[j * ld + i] + Wb[i * ld + j]) * 0.5;
-            Wb[j * ld + i] = s;
-            Wb[i * ld + j] = s;
-            amax = fmax(amax, fabs(s));
-        } else if (i == j) {
-            amax = fmax(amax, fabs(Wb[j * ld + i]));
-        }
+    // P = (P + P^T) / 2 (:309) written straight into layer-0 pair positions
+    // of the ping-pong buffer Vb (leading dimension m); Q is parked in the U
+    // output (global) so that Q's buffer can be the second ping-pong buffer.
+    const int m = (n % 2 == 0) ? n : n + 1;
+    for (int x = t.tid; x < m; x += t.nthreads) {
+        // layer 0: pair k = (m-1, 0) for k = 0, else (k, m-1-k) in ring m-1
+        const int k = x >> 1;
+        int a = k == 0 ? m - 1 : k, bb = k == 0 ? 0 : (m - 1 - k) % (m - 1);
+        const int lo = min(a, bb), hi = max(a, bb);
+        sc->pidx[0][x] = (x & 1) ? hi : lo;
     }
-    amax = team_max(t, amax, sc->red);
-    // Power-of-two column scaling keeps the squared Gram entries of the
-    // one-sided sweep inside the f64 range (exact, undone on sigma).
-    const double wscale = amax > 0.0 ? ldexp(1.0, -ilogb(amax)) : 1.0;
+    for (int idx = t.tid; idx < n * n; idx += t.nthreads) {
+        const int i = idx / n, j = idx % n;
+        job.U[i * job.ldu + j] = Q[j * ld + i];
+    }
+    t.sync();
+    double pf2 = 0.0;
+    for (int idx = t.tid; idx < m * m; idx += t.nthreads) {
+        const int x = idx % m, y = idx / m;
+        const int i = sc->pidx[0][x], j = sc->pidx[0][y];
+        double v = 0.0;
+        if (i < n && j < n) v = (Wb[j * ld + i] + Wb[i * ld + j]) * 0.5;
+        Vb[y * m + x] = v;
+        pf2 = fma(v, v, pf2);
+    }
+    const double pref = fmax(sqrt(team_sum(t, pf2, sc->red)), 1e-300);  // syncs Vb
+    // V = I in the (now free) W buffer; P ping-pongs between Vb and Q's buffer
+    double* Vn = Wb;
     for (int idx = t.tid; idx < np * np; idx += t.nthreads) {
         const int i = idx % np, j = idx / np;
-        Wb[j * ld + i] = (i < n && j < n) ? Wb[j * ld + i] * wscale : 0.0;
-        Vb[j * ld + i] = (i == j && i < n) ? 1.0 : 0.0;
+        Vn[j * ld + i] = (i == j && i < n) ? 1.0 : 0.0;
     }
-    if (t.tid < 4) sc->cnt[t.tid] = 0;
     if (t.tid == 0) sc->rotor_idx = 0;
     t.sync();
 
-    // ---- 3. round-robin one-sided Jacobi on P
-    const int m = (n % 2 == 0) ? n : n + 1;
-    const int layers = (n % 2 == 0) ? (n > 0 ? n - 1 : 0) : n;  // round_robin_layer_count
-    const int max_sweeps = 60 + 20 * n;                           // eigh_jacobi_full, :216
-    const double jtol = sqrt(double(n)) * 2.220446049250313e-16;
-    int sweeps = 0;
+    // ---- 3. two-sided round-robin Jacobi eigensolve of P (eigh_jacobi_full)
     long long rotations = 0;
-    for (int sw = 0; sw < max_sweeps; ++sw) {
-        const int slot = sw & 3;
-        if (t.tid == 0) sc->cnt[(sw + 2) & 3] = 0;
-        sweeps = sw + 1;
-        for (int layer = 0; layer < layers; ++layer) {
-            jacobi_layer<G>(t, n, m, layer, Wb, Vb, ld, jtol, sc, slot, job,
-                            uint32_t(sw * layers + layer));
-            t.sync();
-        }
-        const int rotated = sc->cnt[slot];
-        rotations += rotated;
-        if (rotated == 0) break;
-        if (sw + 1 == max_sweeps) flags |= LSVD_MAT_JACOBI_CAP;
-    }
+    bool jcap = false;
+    double* Pfin = nullptr;
+    int par = 0;
+    const int sweeps = jacobi2pp_sweeps(t, n, Vb, Q, Vn, ld, pref, 60 + 20 * n /* :216 */, sc, job,
+                                        &rotations, &jcap, &Pfin, &par);
+    if (jcap) flags |= LSVD_MAT_JACOBI_CAP;
+    double* const Pother = (Pfin == Vb) ? Q : Vb;
+    Vb = Vn;
 
-    // ---- sigma = column norms, descending stable sort
-    {
-        const int gpw = 32 / G;
-        for (int base = t.warp * gpw; base < n; base += t.nwarps * gpw) {
-            const int j = base + t.lane / G;
-            double s = 0.0;
-            for (int row = t.lane % G; row < n; row += G) {
-                const double w = j < n ? Wb[j * ld + row] : 0.0;
-                s = fma(w, w, s);
-            }
-            s = group_sum<G>(s);
-            if (j < n && t.lane % G == 0) sc->sig[j] = sqrt(s) / wscale;
-        }
+    // ---- eigenvalues on the diagonal, stable descending sort, sigma = max(eig, 0)
+    for (int x = t.tid; x < m; x += t.nthreads) {
+        const int i = sc->pidx[par][x];
+        if (i < n) sc->sig[i] = Pfin[x * m + x];
     }
     t.sync();
     for (int j = t.tid; j < n; j += t.nthreads) {
         const double sj = sc->sig[j];
-        const double kj = isnan(sj) ? -1.0 : sj;
+        const double kj = isnan(sj) ? -INFINITY : sj;
         int rank = 0;
         for (int k = 0; k < n; ++k) {
             const double sk = sc->sig[k];
-            const double kk = isnan(sk) ? -1.0 : sk;
+            const double kk = isnan(sk) ? -INFINITY : sk;
             rank += (kk > kj) || (kk == kj && k < j);
         }
         sc->perm[rank] = j;
     }
     t.sync();
+    for (int j = t.tid; j < n; j += t.nthreads) sc->sig[j] = fmax(sc->sig[j], 0.0);
+    // both ping-pong buffers are free again: Q comes back from the U output
+    double* Ub = Pfin;
+    Q = (Pfin == Q) ? Pother : Q;
+    t.sync();
+    for (int idx = t.tid; idx < np * np; idx += t.nthreads) {
+        const int i = idx / np, j = idx - (idx / np) * np;
+        Q[j * ld + i] = (i < n && j < n) ? job.U[i * job.ldu + j] : 0.0;
+    }
+    t.sync();
     const int* perm = sc->perm;
-
     // ---- 4. U = Q V (sorted); orthogonality check (:317-318)
-    double* Ub = Wb;  // W is no longer needed
     team_gemm<TS>(
         t, np, n, [&](int k, int i) { return Q[k * ld + i]; },
         [&](int k, int j) { return j < n ? Vb[perm[j] * ld + k] : 0.0; },

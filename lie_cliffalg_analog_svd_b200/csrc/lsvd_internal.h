@@ -56,6 +56,7 @@ struct BatchPlan {
     int64_t a_elems = 0, s_elems = 0;
     int n_items = 0;
     int smem_bytes = 0;
+    lsvd_precision precision = LSVD_PREC_FP64;
     // device metadata
     DeviceBuffer d_meta, d_scratch;
     int32_t* m_n = nullptr;
@@ -103,7 +104,7 @@ lsvd_status lsvd_single_small(lsvd_context* ctx, int64_t n, const double* A, int
                               double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
                               lsvd_diag* diag, lsvd_rotor* rotors, int64_t rotor_cap,
                               int64_t* rotor_count, int32_t* perm, uint32_t flags,
-                              int extra_flags);
+                              int extra_flags, bool host_meta);
 
 // lsvd_autotune.cu
 void lsvd_autotune_shapes(lsvd_context* ctx, lsvd_precision prec, ClassShape* shapes);

@@ -3,6 +3,7 @@
 
 #include "lsvd_device.cuh"
 #include "lsvd_internal.h"
+#include "lsvd_mixed.cuh"
 
 namespace lsvd {
 
@@ -131,7 +132,7 @@ __device__ __forceinline__ bool micro_one(int n, const double* A, double* U, dou
 // atomic queue until it drains.  Micro items: one matrix per thread.  Small
 // items: teams of W warps, one matrix per team at a time.
 __global__ void __launch_bounds__(kCtaThreads, 2) batched_kernel(const BatchArgs args) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     __shared__ int s_item;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(args.head, 1);
@@ -177,9 +178,69 @@ __global__ void __launch_bounds__(kCtaThreads, 2) batched_kernel(const BatchArgs
     }
 }
 
+template <int PREC>
+__device__ __forceinline__ void dispatch_mixed(int variant, const Team& t, const SmallJob& job,
+                                               double* sm) {
+    switch (variant) {
+        case 1: mixed_solve_team<2, 16, PREC>(t, job, sm); break;
+        case 3: case 4: case 5: mixed_solve_team<4, 8, PREC>(t, job, sm); break;
+        default: mixed_solve_team<2, 8, PREC>(t, job, sm); break;
+    }
+}
+
+// Persistent batched kernel of the mixed-precision path (same work queue and
+// size classes as batched_kernel; n <= 4 keeps the FP64 micro kernel).
+template <int PREC>
+__global__ void __launch_bounds__(kCtaThreads, 2) batched_mixed_kernel(const BatchArgs args) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(args.head, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= args.n_items) break;
+        const Item item = args.items[it];
+        const ClassCfg cfg = args.cls[item.cls];
+        if (cfg.nwarps == 0) {
+            const int t = threadIdx.x;
+            if (t < item.count) {
+                const int mi = args.perm[item.first + t];
+                const int n = args.n[mi];
+                const int64_t ao = args.aoff[mi], so = args.soff[mi];
+                const bool ok = micro_one(n, args.A + ao, args.U + ao, args.S + so, args.Vt + ao,
+                                          args.diag ? args.diag + mi : nullptr,
+                                          args.want_diag != 0, args.agg_flags);
+                if (!ok) {
+                    const int slot = atomicAdd(args.fb_count, 1);
+                    args.fb_list[slot] = mi;
+                }
+            }
+        } else {
+            const int tsize = 32 * cfg.nwarps;
+            const int teams = kCtaThreads / tsize;
+            const int team = threadIdx.x / tsize;
+            Team tm;
+            tm.tid = threadIdx.x % tsize;
+            tm.nthreads = tsize;
+            tm.warp = tm.tid / 32;
+            tm.lane = threadIdx.x % 32;
+            tm.nwarps = cfg.nwarps;
+            tm.bar = 1 + team;
+            double* sm = smem + size_t(team) * cfg.slice;
+            for (int k = team; k < item.count; k += teams) {
+                const int mi = args.perm[item.first + k];
+                SmallJob job = make_job(args, mi);
+                dispatch_mixed<PREC>(cfg.variant, tm, job, sm);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // Escalations from the micro kernel (rare): LieSvdSmall on a whole CTA.
 __global__ void __launch_bounds__(kCtaThreads, 1) fallback_kernel(const BatchArgs args) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     const int cnt = *args.fb_count;
     Team tm;
     tm.tid = threadIdx.x;
@@ -201,7 +262,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) fallback_kernel(const BatchArg
 // with the rotor stream and sort permutation outputs.
 template <int TS, int G>
 __global__ void __launch_bounds__(kCtaThreads, 1) single_kernel(SmallJob job) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     Team tm;
     tm.tid = threadIdx.x;
     tm.nthreads = kCtaThreads;

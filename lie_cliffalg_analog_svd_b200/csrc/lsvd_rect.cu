@@ -98,7 +98,7 @@ extern "C" lsvd_status lsvd_small_solve_rectangular_f64(lsvd_context* ctx, int64
         return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "solve_rectangular: bad pointer or leading dimension");
     if (m == d)
         return lsvd_single_small(ctx, m, A, lda, U, ldu, S, Vt, ldvt, diag, nullptr, 0, nullptr,
-                                 nullptr, flags, 0);
+                                 nullptr, flags, 0, false);
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
     const bool dev = (flags & LSVD_DEVICE_POINTERS) != 0;
@@ -122,20 +122,25 @@ extern "C" lsvd_status lsvd_small_solve_rectangular_f64(lsvd_context* ctx, int64
     const int64_t rs = wide ? 1 : d, cs = wide ? d : 1;
     const size_t smem = size_t(mm) * 8;
     if (smem > 200 * 1024) return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "solve_rectangular: too many rows");
-    cudaFuncSetAttribute(qr_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if ((e = cudaFuncSetAttribute(qr_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem))) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "qr smem attribute");
     qr_reduce_kernel<<<1, kCtaThreads, smem, st>>>(mm, dd, dA, rs, cs, dQ, dR);
     ctx->launches++;
     if ((e = cudaGetLastError()) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "qr_reduce");
     // square solve of R (device pointers, synchronous)
     lsvd_diag local;
     lsvd_status s2 = lsvd_single_small(ctx, dd, dR, dd, dUr, dd, dS, dVr, dd, &local, nullptr, 0,
-                                       nullptr, nullptr, LSVD_DEVICE_POINTERS | (flags & LSVD_WANT_DIAG), 0);
+                                       nullptr, nullptr, LSVD_DEVICE_POINTERS | (flags & LSVD_WANT_DIAG), 0,
+                                       true);
     if (s2 != LSVD_OK && s2 != LSVD_NOT_CONVERGED && s2 != LSVD_NONFINITE_INPUT) return s2;
     if (diag) {
-        if (dev)
-            cudaMemcpy(diag, &local, sizeof(local), cudaMemcpyHostToDevice);
-        else
+        if (dev) {
+            if ((e = cudaMemcpy(diag, &local, sizeof(local), cudaMemcpyHostToDevice)) != cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "copy diag out");
+        } else {
             *diag = local;
+        }
     }
     // outputs: tall: U = Q U_r (m x k), Vt = Vt_r (k x d)
     //          wide: SVD(A^T) = (Q U_r, s, Vt_r) -> U = Vt_r^T (m x m), Vt = (Q U_r)^T (k x d)
