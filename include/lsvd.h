@@ -152,6 +152,29 @@ LSVD_API lsvd_status lsvd_svd_batched_f64(lsvd_context* ctx, int64_t count, cons
                                           lsvd_diag* diags, lsvd_precision precision,
                                           uint32_t flags);
 
+/* No counterpart in the reference.  The batched FP64 SVD of
+ * lsvd_svd_batched_f64 for callers that cannot allocate device memory: code
+ * running while its stream is captured into a CUDA graph (cudaMalloc is not
+ * allowed there), latency-critical loops that cannot absorb the device-wide
+ * synchronisation of cudaMalloc/cudaFree, and hosts whose device memory
+ * belongs to their own allocator or pool.  It allocates nothing: A, U, S, Vt
+ * (and diags, may be NULL) are DEVICE buffers of the caller in the packed
+ * layout of lsvd_svd_batched_f64, `n` is host memory, `stream` a
+ * cudaStream_t of the current device (NULL = legacy default stream), and all
+ * working memory is a static device array of LSVD_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until exit.  At most
+ * LSVD_NOALLOC_MAX_COUNT matrices per call (more returns LSVD_UNSUPPORTED).
+ * The first call on a device sets that device up (symbol address, kernel
+ * attributes): make it before any stream capture.  Calls share the static
+ * array, so calls that overlap on a GPU race; serialise them.  With
+ * LSVD_ASYNC the call only enqueues work; otherwise it synchronises `stream`
+ * and reports the outcome like lsvd_svd_batched_f64. */
+#define LSVD_NOALLOC_MAX_COUNT 65536
+#define LSVD_NOALLOC_SCRATCH_BYTES (4096 + 44 * LSVD_NOALLOC_MAX_COUNT)
+LSVD_API lsvd_status lsvd_svd_batched_noalloc_f64(void* stream, int64_t count, const int32_t* n,
+                                                  const double* A, double* U, double* S,
+                                                  double* Vt, lsvd_diag* diags, uint32_t flags);
+
 /* Replaces metrics::compute (src/lib.rs:149-194) for one matrix (general
  * thin shape: A m*d, U m*k, S k, Vt k*d).  out[0..4] = rel_recon, orth_u,
  * orth_v, sigma_max_rel, sigma_tail_rel (NaN when sigma_ref is NULL). */

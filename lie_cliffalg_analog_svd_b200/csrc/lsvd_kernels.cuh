@@ -128,6 +128,7 @@ __device__ __forceinline__ bool micro_one(int n, const double* A, double* U, dou
     return true;
 }
 
+#ifndef LSVD_KERNELS_DEVICE_ONLY
 // Persistent batched kernel: CTAs pull work items (largest n first) from an
 // atomic queue until it drains.  Micro items: one matrix per thread.  Small
 // items: teams of W warps, one matrix per team at a time.
@@ -280,5 +281,7 @@ __global__ void micro_single_kernel(int n, const double* A, double* U, double* S
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     *need_fallback = micro_one(n, A, U, S, Vt, diag, want_diag != 0, agg) ? 0 : 1;
 }
+
+#endif  // LSVD_KERNELS_DEVICE_ONLY
 
 }  // namespace lsvd
