@@ -183,6 +183,39 @@ LSVD_API lsvd_status lsvd_metrics_f64(lsvd_context* ctx, int64_t m, int64_t d, i
                                       const double* Vt, const double* sigma_ref, double* out,
                                       uint32_t flags);
 
+/* --------------------------------------------------------- Phase-JADE ---- */
+
+/* JointDiagonalizationParams (src/lie_svd_joint.rs:18-35). */
+typedef struct lsvd_joint_params {
+    int32_t max_sweeps;
+    double tol;
+    double min_pair_scale;
+    int32_t line_search_steps;
+} lsvd_joint_params;
+
+/* JointDiagonalizationTrace (src/lie_svd_joint.rs:43-50). */
+typedef struct lsvd_joint_trace {
+    double initial_offdiag;
+    double final_offdiag;
+    int64_t sweeps;
+    int64_t rotations;
+    int64_t rejected_rotations;
+} lsvd_joint_trace;
+
+/* JointDiagonalizationParams::for_n (src/lie_svd_joint.rs:27-34). */
+LSVD_API lsvd_joint_params lsvd_joint_params_for_n(int64_t n);
+
+/* Replaces LieSvdJoint::diagonalize_symmetric_with_params
+ * (src/lie_svd_joint.rs:71-158) for `families` independent families at once.
+ * M: families x K matrices of n x n, back to back (row-major); V: families x
+ * n x n (the shared basis, columns = joint eigenvectors); diag: families x K
+ * x n (the diagonals of V^T M_k V); traces: `families` entries, HOST memory
+ * always.  params NULL = lsvd_joint_params_for_n(n).  K in 1..99. */
+LSVD_API lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, int64_t K, int64_t n,
+                                       const double* M, const lsvd_joint_params* params,
+                                       double* V, double* diag, lsvd_joint_trace* traces,
+                                       uint32_t flags);
+
 /* ----------------------------------------------------- rotor schedule ---- */
 /* target: 0 = "mzi_mesh", 1 = "fpga_rotor_mesh" (HardwareTarget,
  * src/lie_svd_compiler.rs:12-25).  The JSON text (NUL-terminated) is written

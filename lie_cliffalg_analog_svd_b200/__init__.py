@@ -7,9 +7,10 @@ API over that ABI.  Importing the package does not load the library;
 the first call does, and fails loudly if it was not built.
 """
 from .api import (Context, LieSvd, LieSvdMicro, LieSvdSmall, SmallResult, SvdMetrics,  # noqa: F401
-                  HardwareSchedule, default_context, metrics, packed_offsets, svd_batched,
+                  HardwareSchedule, JointDiagonalizationParams, LieSvdJoint, default_context,
+                  metrics, packed_offsets, svd_batched,
                   unpack)
 from ._lib import LsvdError  # noqa: F401
 
-__all__ = ["Context", "HardwareSchedule", "LieSvd", "LieSvdMicro", "LieSvdSmall", "SmallResult", "SvdMetrics",
+__all__ = ["Context", "HardwareSchedule", "JointDiagonalizationParams", "LieSvdJoint", "LieSvd", "LieSvdMicro", "LieSvdSmall", "SmallResult", "SvdMetrics",
            "default_context", "metrics", "packed_offsets", "svd_batched", "unpack", "LsvdError"]

@@ -37,6 +37,16 @@ DIAG_DTYPE = [("rel_recon", "<f8"), ("orth_u", "<f8"), ("orth_v", "<f8"), ("ns_i
 ROTOR_DTYPE = [("i", "<u2"), ("j", "<u2"), ("round", "<u4"), ("theta", "<f8")]
 
 
+class JointParams(C.Structure):
+    _fields_ = [("max_sweeps", C.c_int32), ("tol", C.c_double), ("min_pair_scale", C.c_double),
+                ("line_search_steps", C.c_int32)]
+
+
+class JointTrace(C.Structure):
+    _fields_ = [("initial_offdiag", C.c_double), ("final_offdiag", C.c_double),
+                ("sweeps", C.c_int64), ("rotations", C.c_int64), ("rejected_rotations", C.c_int64)]
+
+
 class LsvdError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"lsvd status {status}: {msg}")
@@ -66,6 +76,8 @@ SIGNATURES = {
     "lsvd_svd_batched_f64": (C.c_int, [P, I64, P, P, P, P, P, P, C.c_int, U32]),
     "lsvd_metrics_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, P, U32]),
     "lsvd_svd_batched_noalloc_f64": (C.c_int, [P, I64, P, P, P, P, P, P, U32]),
+    "lsvd_joint_params_for_n": (JointParams, [I64]),
+    "lsvd_jade_sym_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, U32]),
     "lsvd_schedule_from_orthogonal": (C.c_int, [I64, P, C.c_int32, P, I64, C.POINTER(I64)]),
     "lsvd_schedule_from_rotors": (C.c_int, [P, I64, I64, C.c_int32, P, I64, C.POINTER(I64)]),
 }

@@ -329,3 +329,70 @@ class HardwareSchedule:
         lib = L.load()
         return _json_call(lib.lsvd_schedule_from_rotors, _ptr(r) if r.size else None, r.size,
                           channels, TARGETS[target])
+
+
+@dataclass
+class JointDiagonalizationParams:
+    """``JointDiagonalizationParams`` (src/lie_svd_joint.rs:18-41)."""
+    max_sweeps: int
+    tol: float = 1e-12
+    min_pair_scale: float = 1e-14
+    line_search_steps: int = 6
+
+    @staticmethod
+    def for_n(n: int) -> "JointDiagonalizationParams":
+        return JointDiagonalizationParams(max_sweeps=12 + max(n, 1))
+
+
+@dataclass
+class JointDiagonalizationTrace:
+    initial_offdiag: float
+    final_offdiag: float
+    sweeps: int
+    rotations: int
+    rejected_rotations: int
+
+
+class LieSvdJoint:
+    """``LieSvdJoint`` symmetric route (src/lie_svd_joint.rs:61-158) on the GPU,
+    plus a batched form over independent families."""
+
+    @staticmethod
+    def diagonalize_symmetric(matrices, ctx: Context | None = None):
+        n = np.asarray(matrices[0]).shape[0] if len(matrices) else 0
+        return LieSvdJoint.diagonalize_symmetric_with_params(
+            matrices, JointDiagonalizationParams.for_n(n), ctx=ctx)
+
+    @staticmethod
+    def diagonalize_symmetric_with_params(matrices, params: JointDiagonalizationParams,
+                                          ctx: Context | None = None):
+        if len(matrices) == 0:
+            raise L.LsvdError(L.BAD_SHAPE, "LieSvdJoint: empty matrix set")
+        m = _f64(np.stack([np.asarray(x, dtype=np.float64) for x in matrices]))
+        if m.ndim != 3 or m.shape[1] != m.shape[2]:
+            raise L.LsvdError(L.BAD_SHAPE, "LieSvdJoint: matrices must be square")
+        v, d, tr = LieSvdJoint.diagonalize_families(m[None], params, ctx=ctx)
+        return v[0], [d[0, k].copy() for k in range(m.shape[0])], tr[0]
+
+    @staticmethod
+    def diagonalize_families(m, params: JointDiagonalizationParams | None = None,
+                             ctx: Context | None = None):
+        """``m``: (families, K, n, n).  Returns V (families, n, n), diagonals
+        (families, K, n) and one trace per family."""
+        ctx = ctx or default_context()
+        m = _f64(m)
+        F, K, n, n2 = m.shape
+        if n != n2:
+            raise L.LsvdError(L.BAD_SHAPE, "LieSvdJoint: matrices must be square")
+        v = np.empty((F, n, n)); d = np.empty((F, K, n))
+        tr = (L.JointTrace * F)()
+        p = None
+        if params is not None:
+            p = L.JointParams(params.max_sweeps, params.tol, params.min_pair_scale,
+                              params.line_search_steps)
+        st = ctx.lib.lsvd_jade_sym_f64(ctx.handle, F, K, n, _ptr(m), C.byref(p) if p else None,
+                                       _ptr(v), _ptr(d), tr, 0)
+        _check(ctx.lib, ctx.handle, st, "LieSvdJoint::diagonalize_symmetric")
+        traces = [JointDiagonalizationTrace(t.initial_offdiag, t.final_offdiag, t.sweeps,
+                                            t.rotations, t.rejected_rotations) for t in tr]
+        return v, d, traces

@@ -1,0 +1,529 @@
+// lsvd_jade.cu -- Phase-JADE joint diagonalisation of symmetric families,
+// LieSvdJoint::diagonalize_symmetric_with_params (src/lie_svd_joint.rs:71-158),
+// batched over independent families.
+//
+// One family is K matrices of n x n; the reference sweeps n-1 round-robin
+// layers (layer_pairs, :524-539) of disjoint index pairs, and for each pair
+//   * skips it if sum_k |m_ij| + |m_ji| <= pair_tol              (:118)
+//   * takes the Cardoso angle 1/4 atan2(2 sxy, syy - sxx), or its pi/4
+//     alternative if that leaves less 2x2 off-diagonal energy   (:338-357)
+//   * skips |theta| <= 1e-18                                      (:122)
+//   * applies the symmetric rotor to all K matrices and accepts it if the
+//     local off-diagonal energy does not grow beyond 1e-14 max(before, 1),
+//     else rolls back and halves theta, line_search_steps times (:359-386)
+// and stops a sweep loop when the joint off-diagonal norm is <= tol or
+// stopped decreasing by 1e-10 (:139-142).
+//
+// Blocked on the GPU: indices are cut into blocks of B = 8 and the blocks are
+// paired by the same circle method; for each block pair the K principal
+// 16 x 16 sub-blocks are staged in shared memory (jade_solve_kernel) and every
+// index pair inside is treated by the rules above -- cross pairs in every
+// block layer, pairs inside a block in block layer 0, so each index pair is
+// visited once per sweep, as in the reference.  The accepted rotations of a
+// block pair compose into one 16 x 16 orthogonal R, and a second pass
+// (jade_apply_kernel) applies all of a layer's R to every 16 x 16 tile of
+// every matrix, M[P,Q] <- R_P^T M[P,Q] R_Q, and to V: the family is streamed
+// once per block layer instead of once per index layer.
+//
+// The acceptance test uses the exact change of the pair's 2 x 2 block energy
+// (the energy of rows/columns i, j outside the block is invariant under the
+// pair's rotation) and the sub-block's local energy for the slack, so it
+// differs from the reference only in rounding (decisions are identical in
+// exact arithmetic); the pair order inside a sweep differs, so parity is on
+// the converged result (final off-diagonal, V orthogonality, diagonals).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "lsvd.h"
+#include "lsvd_internal.h"
+
+namespace {
+
+constexpr int B = 8;        // block size
+constexpr int B2 = 2 * B;   // indices of a block pair
+constexpr int kThreads = 256;
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double wrap_quarter(double a) {  // wrap_jacobi_angle, :506-514
+    while (a > 0.25 * kPi) a -= 0.5 * kPi;
+    while (a < -0.25 * kPi) a += 0.5 * kPi;
+    return a;
+}
+
+__device__ __forceinline__ void rr_pair(int m, int layer, int k, int& a, int& b) {
+    const int ring = m - 1;
+    if (k == 0) {
+        a = m - 1;
+        b = layer % ring;
+    } else {
+        a = (layer + k) % ring;
+        b = (layer + ring - k) % ring;
+    }
+}
+
+struct JadeArgs {
+    int F, K, n, nbe;        // families, matrices per family, order, blocks (even)
+    int layer;               // block layer
+    int steps;               // line_search_steps
+    const double* pair_tol;  // per family
+    double* W;               // F*K*n*n, rotated in place
+    double* V;               // F*n*n
+    double* R;               // F*(nbe/2)*B2*B2
+    long long* rot;          // per family: accepted, rejected
+    const int* active;       // per family
+};
+
+// Block pair (A, Bk) of `layer` -> the 16 global indices (B of block A, then
+// B of block Bk); -1 marks padding past n.
+__device__ __forceinline__ void block_indices(const JadeArgs& a, int bp, int* idx) {
+    int A, Bb;
+    rr_pair(a.nbe, a.layer, bp, A, Bb);
+    const int lo = min(A, Bb), hi = max(A, Bb);
+    for (int t = 0; t < B; ++t) {
+        const int i0 = lo * B + t, i1 = hi * B + t;
+        idx[t] = i0 < a.n ? i0 : -1;
+        idx[B + t] = i1 < a.n ? i1 : -1;
+    }
+}
+
+// grid (nbe/2, F).  Shared: K x 16 x 16 sub-blocks + R + pair tables.
+__global__ void __launch_bounds__(kThreads, 1) jade_solve_kernel(JadeArgs a) {
+    extern __shared__ __align__(16) double sh[];
+    const int bp = blockIdx.x, f = blockIdx.y;
+    const int nbp = a.nbe / 2;
+    double* R = a.R + (size_t(f) * nbp + bp) * B2 * B2;
+    __shared__ int idx[B2];
+    __shared__ int pl[B], pm[B];          // pairs of the current round (local indices)
+    __shared__ double pc[B], ps[B];       // accepted rotation (cos, sin), s = 0: none
+    __shared__ long long nacc, nrej;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (!a.active[f]) {
+        // keep R = I so the apply pass is a no-op for finished families
+        for (int e = tid; e < B2 * B2; e += kThreads) R[e] = (e / B2 == e % B2) ? 1.0 : 0.0;
+        return;
+    }
+    if (tid == 0) {
+        block_indices(a, bp, idx);
+        nacc = 0;
+        nrej = 0;
+    }
+    __syncthreads();
+    const int K = a.K, n = a.n;
+    double* S = sh;                    // S[k][r][c]
+    double* Rs = sh + size_t(K) * B2 * B2;
+    const double* Wf = a.W + size_t(f) * K * n * n;
+    for (int e = tid; e < K * B2 * B2; e += kThreads) {
+        const int k = e / (B2 * B2), r = (e / B2) % B2, c = e % B2;
+        const int gi = idx[r], gj = idx[c];
+        S[e] = (gi >= 0 && gj >= 0) ? Wf[(size_t(k) * n + gi) * n + gj] : 0.0;
+    }
+    for (int e = tid; e < B2 * B2; e += kThreads) Rs[e] = (e / B2 == e % B2) ? 1.0 : 0.0;
+    __syncthreads();
+    const double ptol = a.pair_tol[f];
+    const int rounds_cross = B, rounds_intra = (a.layer == 0) ? B - 1 : 0;
+    for (int round = 0; round < rounds_cross + rounds_intra; ++round) {
+        if (tid < B) {
+            int l, m;
+            if (round < rounds_cross) {  // cross pairs (t, B + (t + round) % B)
+                l = tid;
+                m = B + (tid + round) % B;
+            } else {  // pairs inside each block: round robin over B, I and J at once
+                const int rr = round - rounds_cross, k = tid % (B / 2);
+                int x, y;
+                rr_pair(B, rr, k, x, y);
+                const int off = tid < B / 2 ? 0 : B;
+                l = off + min(x, y);
+                m = off + max(x, y);
+            }
+            pl[tid] = l;
+            pm[tid] = m;
+            pc[tid] = 1.0;
+            ps[tid] = 0.0;
+        }
+        __syncthreads();
+        // one warp per pair: angle, line search over the K matrices
+        if (warp < B) {
+            const int li = pl[warp], lj = pm[warp];
+            const bool valid = idx[li] >= 0 && idx[lj] >= 0;
+            double poff = 0.0, sxx = 0.0, syy = 0.0, sxy = 0.0;
+            if (valid)
+                for (int k = lane; k < K; k += 32) {
+                    const double* Sk = S + size_t(k) * B2 * B2;
+                    const double mij = Sk[li * B2 + lj], mji = Sk[lj * B2 + li];
+                    poff += fabs(mij) + fabs(mji);
+                    const double x = 0.5 * (Sk[li * B2 + li] - Sk[lj * B2 + lj]);
+                    const double y = 0.5 * (mij + mji);
+                    sxx += x * x;
+                    syy += y * y;
+                    sxy += x * y;
+                }
+            poff = warp_sum(poff);
+            sxx = warp_sum(sxx);
+            syy = warp_sum(syy);
+            sxy = warp_sum(sxy);
+            if (valid && poff > ptol) {
+                double th = 0.25 * atan2(2.0 * sxy, syy - sxx);
+                const double alt = wrap_quarter(th + 0.25 * kPi);
+                th = wrap_quarter(th);
+                // joint_pair_energy_after (:388-399) for both candidates
+                double st, ct, sa, ca;
+                sincos(th, &st, &ct);
+                sincos(alt, &sa, &ca);
+                double et = 0.0, ea = 0.0, before = 0.0;
+                for (int k = lane; k < K; k += 32) {
+                    const double* Sk = S + size_t(k) * B2 * B2;
+                    const double av = Sk[li * B2 + li], dv = Sk[lj * B2 + lj];
+                    const double bv = 0.5 * (Sk[li * B2 + lj] + Sk[lj * B2 + li]);
+                    const double ot = 0.5 * (av - dv) * (2.0 * st * ct) + bv * (ct * ct - st * st);
+                    const double oa = 0.5 * (av - dv) * (2.0 * sa * ca) + bv * (ca * ca - sa * sa);
+                    et += 2.0 * ot * ot;
+                    ea += 2.0 * oa * oa;
+                    // local_offdiag_sq_for_axes (:475-494) restricted to the sub-block
+                    for (int c = 0; c < B2; ++c) {
+                        if (c != li) before += Sk[li * B2 + c] * Sk[li * B2 + c];
+                        if (c != lj) before += Sk[lj * B2 + c] * Sk[lj * B2 + c];
+                        if (c != li && c != lj)
+                            before += Sk[c * B2 + li] * Sk[c * B2 + li] + Sk[c * B2 + lj] * Sk[c * B2 + lj];
+                    }
+                }
+                et = warp_sum(et);
+                ea = warp_sum(ea);
+                before = warp_sum(before);
+                const double theta = ea < et ? alt : th;
+                if (fabs(theta) > 1e-18) {
+                    // accept_joint_rotor (:359-386): the rotor changes the local
+                    // energy only through the pair's 2x2 block
+                    const double slack = 1e-14 * fmax(before, 1.0);
+                    double scale = 1.0, cacc = 1.0, sacc = 0.0;
+                    bool ok = false;
+                    for (int stp = 0; stp < max(a.steps, 1); ++stp) {
+                        double s, c;
+                        sincos(theta * scale, &s, &c);
+                        double delta = 0.0;
+                        for (int k = lane; k < K; k += 32) {
+                            const double* Sk = S + size_t(k) * B2 * B2;
+                            const double m00 = Sk[li * B2 + li], m01 = Sk[li * B2 + lj];
+                            const double m10 = Sk[lj * B2 + li], m11 = Sk[lj * B2 + lj];
+                            // rows then columns (apply_symmetric_rotor, :401-404)
+                            const double r00 = c * m00 - s * m10, r01 = c * m01 - s * m11;
+                            const double r10 = s * m00 + c * m10, r11 = s * m01 + c * m11;
+                            const double n01 = s * r00 + c * r01;
+                            const double n10 = c * r10 - s * r11;
+                            delta += n01 * n01 + n10 * n10 - m01 * m01 - m10 * m10;
+                        }
+                        delta = warp_sum(delta);
+                        const double after = before + delta;
+                        if (after <= before + slack && isfinite(after)) {
+                            ok = true;
+                            cacc = c;
+                            sacc = s;
+                            break;
+                        }
+                        scale *= 0.5;
+                    }
+                    if (lane == 0) {
+                        if (ok) {
+                            pc[warp] = cacc;
+                            ps[warp] = sacc;
+                            atomicAdd((unsigned long long*)&nacc, 1ull);
+                        } else {
+                            atomicAdd((unsigned long long*)&nrej, 1ull);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // rows (apply_left_rotor, :406-415) of every pair in the round
+        for (int e = tid; e < B * K * B2; e += kThreads) {
+            const int p = e / (K * B2), k = (e / B2) % K, col = e % B2;
+            const double s = ps[p];
+            if (s == 0.0) continue;
+            const double c = pc[p];
+            double* Sk = S + size_t(k) * B2 * B2;
+            const int li = pl[p], lj = pm[p];
+            const double x = Sk[li * B2 + col], y = Sk[lj * B2 + col];
+            Sk[li * B2 + col] = c * x - s * y;
+            Sk[lj * B2 + col] = s * x + c * y;
+        }
+        __syncthreads();
+        // columns (apply_right_rotor, :417-426) and the basis (apply_basis_rotor, :428-437)
+        for (int e = tid; e < B * (K + 1) * B2; e += kThreads) {
+            const int p = e / ((K + 1) * B2), k = (e / B2) % (K + 1), row = e % B2;
+            const double s = ps[p];
+            if (s == 0.0) continue;
+            const double c = pc[p];
+            double* Sk = k < K ? S + size_t(k) * B2 * B2 : Rs;
+            const int li = pl[p], lj = pm[p];
+            const double x = Sk[row * B2 + li], y = Sk[row * B2 + lj];
+            Sk[row * B2 + li] = c * x - s * y;
+            Sk[row * B2 + lj] = s * x + c * y;
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < B2 * B2; e += kThreads) R[e] = Rs[e];
+    if (tid == 0) {
+        atomicAdd((unsigned long long*)&a.rot[2 * f], (unsigned long long)nacc);
+        atomicAdd((unsigned long long*)&a.rot[2 * f + 1], (unsigned long long)nrej);
+    }
+}
+
+// grid (nbp, K + 1, F): row block pair P of matrix k (k == K: the basis V).
+// Every tile M[P, Q] <- R_P^T M[P, Q] R_Q (for V: V[:, Q] <- V[:, Q] R_Q).
+__global__ void __launch_bounds__(kThreads) jade_apply_kernel(JadeArgs a) {
+    const int P = blockIdx.x, k = blockIdx.y, f = blockIdx.z;
+    if (!a.active[f]) return;
+    const int nbp = a.nbe / 2, n = a.n;
+    __shared__ double RP[B2 * B2], RQ[B2 * B2], T[B2 * B2], X[B2 * B2];
+    __shared__ int ip[B2], iq[B2];
+    const int tid = threadIdx.x, r = tid / B2, c = tid % B2;
+    const bool isV = k == a.K;
+    double* M = isV ? a.V + size_t(f) * n * n : a.W + (size_t(f) * a.K + k) * n * n;
+    if (tid < B2) {
+        int A, Bb;
+        rr_pair(a.nbe, a.layer, P, A, Bb);
+        const int lo = min(A, Bb), hi = max(A, Bb);
+        const int t = tid % B;
+        const int g = (tid < B ? lo : hi) * B + t;
+        ip[tid] = g < n ? g : -1;
+    }
+    RP[tid] = a.R[(size_t(f) * nbp + P) * B2 * B2 + tid];
+    __syncthreads();
+    for (int Q = 0; Q < nbp; ++Q) {
+        if (tid < B2) {
+            int A, Bb;
+            rr_pair(a.nbe, a.layer, Q, A, Bb);
+            const int lo = min(A, Bb), hi = max(A, Bb);
+            const int t = tid % B;
+            const int g = (tid < B ? lo : hi) * B + t;
+            iq[tid] = g < n ? g : -1;
+        }
+        RQ[tid] = a.R[(size_t(f) * nbp + Q) * B2 * B2 + tid];
+        __syncthreads();
+        const int gi = ip[r], gj = iq[c];
+        X[tid] = (gi >= 0 && gj >= 0) ? M[size_t(gi) * n + gj] : 0.0;
+        __syncthreads();
+        double t = 0.0;
+        for (int x = 0; x < B2; ++x) t = fma(X[r * B2 + x], RQ[x * B2 + c], t);
+        T[tid] = t;
+        __syncthreads();
+        double o;
+        if (isV) {
+            o = t;
+        } else {
+            o = 0.0;
+            for (int y = 0; y < B2; ++y) o = fma(RP[y * B2 + r], T[y * B2 + c], o);
+        }
+        if (gi >= 0 && gj >= 0) M[size_t(gi) * n + gj] = o;
+        __syncthreads();
+    }
+}
+
+// Per family: sum over k, i != j of m_ij^2 (joint_offdiag_norm^2, :439-441)
+// and sum of all squares (joint_frobenius_norm^2, :443-449).
+__global__ void jade_norms_kernel(int F, int K, int n, const double* W, const int* active,
+                                  double* off2, double* all2) {
+    const int f = blockIdx.x;
+    if (active && !active[f]) return;
+    __shared__ double red[2][kThreads / 32];
+    const double* Wf = W + size_t(f) * K * n * n;
+    double so = 0.0, sa = 0.0;
+    const size_t tot = size_t(K) * n * n;
+    for (size_t e = threadIdx.x; e < tot; e += kThreads) {
+        const double v = Wf[e];
+        const size_t ij = e % (size_t(n) * n);
+        sa += v * v;
+        if (ij / n != ij % n) so += v * v;
+    }
+    so = warp_sum(so);
+    sa = warp_sum(sa);
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = so;
+        red[1][threadIdx.x >> 5] = sa;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) {
+            a += red[0][w];
+            b += red[1][w];
+        }
+        off2[f] = a;
+        all2[f] = b;
+    }
+}
+
+__global__ void jade_init_kernel(int F, int n, double* V) {
+    const size_t tot = size_t(F) * n * n;
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < tot;
+         e += size_t(gridDim.x) * blockDim.x) {
+        const size_t ij = e % (size_t(n) * n);
+        V[e] = (ij / n == ij % n) ? 1.0 : 0.0;
+    }
+}
+
+__global__ void jade_diag_kernel(int F, int K, int n, const double* W, double* D) {
+    const size_t tot = size_t(F) * K * n;
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < tot;
+         e += size_t(gridDim.x) * blockDim.x) {
+        const size_t fk = e / n, i = e % n;
+        D[e] = W[fk * n * n + i * n + i];
+    }
+}
+
+}  // namespace
+
+extern "C" lsvd_joint_params lsvd_joint_params_for_n(int64_t n) {
+    lsvd_joint_params p;
+    p.max_sweeps = int32_t(12 + std::max<int64_t>(n, 1));
+    p.tol = 1e-12;
+    p.min_pair_scale = 1e-14;
+    p.line_search_steps = 6;
+    return p;
+}
+
+extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, int64_t K, int64_t n,
+                                         const double* M, const lsvd_joint_params* params,
+                                         double* V, double* diag, lsvd_joint_trace* traces,
+                                         uint32_t flags) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    if (families < 0 || K < 0 || n < 0) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "LieSvdJoint: bad shape");
+    if (families == 0) return LSVD_OK;
+    if (K == 0) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "LieSvdJoint: empty matrix set");
+    if (!M || !V || !diag || !traces) return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "null pointer");
+    const size_t smem = size_t(K) * B2 * B2 * 8 + B2 * B2 * 8;
+    if (smem > 200 * 1024 || n > 32768)
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "LieSvdJoint: K must be <= 99 (shared memory)");
+    const lsvd_joint_params p = params ? *params : lsvd_joint_params_for_n(n);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const bool dev = (flags & LSVD_DEVICE_POINTERS) != 0;
+    const int F = int(families);
+    const size_t wsz = size_t(F) * K * n * n, vsz = size_t(F) * n * n;
+    const int nb = int((n + B - 1) / B), nbe = nb % 2 == 0 ? std::max(nb, 2) : nb + 1;
+    const int nbp = nbe / 2, layers = nbe - 1;
+    cudaError_t e;
+    // workspace: W (work copy) | V | R | off2, all2, tol | rot | active
+    const size_t rsz = size_t(F) * nbp * B2 * B2;
+    auto al = [](size_t x) { return (x + 31) & ~size_t(31); };
+    const size_t bytes = 8 * (al(wsz) + (dev ? 0 : al(vsz)) + al(rsz) + 4 * al(F)) + 16 * al(F) + 4 * al(F);
+    char* ws = static_cast<char*>(ctx->ws_rot.get(bytes, &e));
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "jade workspace");
+    char* q = ws;
+    double* dW = reinterpret_cast<double*>(q); q += 8 * al(wsz);
+    double* dV = dev ? V : reinterpret_cast<double*>(q);
+    if (!dev) q += 8 * al(vsz);
+    double* dR = reinterpret_cast<double*>(q); q += 8 * al(rsz);
+    double* off2 = reinterpret_cast<double*>(q); q += 8 * al(F);
+    double* all2 = reinterpret_cast<double*>(q); q += 8 * al(F);
+    double* ptol = reinterpret_cast<double*>(q); q += 8 * al(F);
+    q += 8 * al(F);
+    long long* rot = reinterpret_cast<long long*>(q); q += 16 * al(F);
+    int* active = reinterpret_cast<int*>(q);
+    if ((e = cudaMemcpyAsync(dW, M, wsz * 8, cudaMemcpyDefault, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(rot, 0, size_t(F) * 16, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "jade setup");
+    jade_init_kernel<<<std::min<size_t>((vsz + 255) / 256, 4096), 256, 0, st>>>(F, int(n), dV);
+    jade_norms_kernel<<<F, kThreads, 0, st>>>(F, int(K), int(n), dW, nullptr, off2, all2);
+    ctx->launches += 2;
+    std::vector<double> h_off(F), h_all(F), h_tol(F), h_ptol(F), h_init(F), h_final(F);
+    std::vector<int> h_act(F, 1);
+    std::vector<long long> h_sweeps(F, 0);
+    if ((e = cudaMemcpyAsync(h_off.data(), off2, 8 * F, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h_all.data(), all2, 8 * F, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "jade norms");
+    for (int f = 0; f < F; ++f) {
+        const double ref = std::max(std::sqrt(h_all[f]), 1e-300);  // :105
+        h_ptol[f] = p.min_pair_scale * std::max(ref, 1.0);        // :106
+        h_tol[f] = p.tol * std::max(ref, 1.0);                    // :107
+        h_init[f] = std::sqrt(h_off[f]);                          // :108
+        if (n <= 1) h_act[f] = 0;                                 // :87-101
+    }
+    if ((e = cudaMemcpyAsync(ptol, h_ptol.data(), 8 * F, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(active, h_act.data(), 4 * F, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "jade upload");
+    if ((e = cudaFuncSetAttribute(jade_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem))) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "jade smem");
+    JadeArgs a;
+    a.F = F;
+    a.K = int(K);
+    a.n = int(n);
+    a.nbe = nbe;
+    a.steps = p.line_search_steps;
+    a.pair_tol = ptol;
+    a.W = dW;
+    a.V = dV;
+    a.R = dR;
+    a.rot = rot;
+    a.active = active;
+    std::vector<double> before(h_init);
+    int live = 0;
+    for (int f = 0; f < F; ++f) live += h_act[f];
+    for (int sw = 0; sw < p.max_sweeps && live > 0; ++sw) {
+        for (int f = 0; f < F; ++f)
+            if (h_act[f]) h_sweeps[f] = sw + 1;
+        for (int l = 0; l < layers; ++l) {
+            a.layer = l;
+            jade_solve_kernel<<<dim3(nbp, F), kThreads, smem, st>>>(a);
+            jade_apply_kernel<<<dim3(nbp, unsigned(K + 1), F), kThreads, 0, st>>>(a);
+            ctx->launches += 2;
+        }
+        jade_norms_kernel<<<F, kThreads, 0, st>>>(F, int(K), int(n), dW, active, off2, all2);
+        ctx->launches++;
+        if ((e = cudaGetLastError()) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "jade sweep");
+        if ((e = cudaMemcpyAsync(h_off.data(), off2, 8 * F, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "jade sweep sync");
+        live = 0;
+        for (int f = 0; f < F; ++f) {
+            if (!h_act[f]) continue;
+            const double after = std::sqrt(h_off[f]);
+            if (after <= h_tol[f] || after >= before[f] * (1.0 - 1e-10)) h_act[f] = 0;  // :139-142
+            before[f] = after;
+            live += h_act[f];
+        }
+        if ((e = cudaMemcpyAsync(active, h_act.data(), 4 * F, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "jade active");
+    }
+    // final_offdiag (:145), diagonals (:146), outputs
+    jade_norms_kernel<<<F, kThreads, 0, st>>>(F, int(K), int(n), dW, nullptr, off2, all2);
+    double* dD = dev ? diag : dR;  // R is dead: reuse it for the diagonals on the host path
+    if (!dev && rsz < size_t(F) * K * n) {
+        dD = reinterpret_cast<double*>(static_cast<char*>(ctx->ws_u.get(size_t(F) * K * n * 8, &e)));
+        if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "jade diag");
+    }
+    jade_diag_kernel<<<std::min<size_t>((size_t(F) * K * n + 255) / 256, 4096), 256, 0, st>>>(
+        F, int(K), int(n), dW, dD);
+    ctx->launches += 2;
+    std::vector<long long> h_rot(2 * size_t(F));
+    if ((e = cudaMemcpyAsync(h_off.data(), off2, 8 * F, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h_rot.data(), rot, 16 * size_t(F), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "jade out");
+    if (!dev) {
+        if ((e = cudaMemcpyAsync(V, dV, vsz * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(diag, dD, size_t(F) * K * n * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "jade copy out");
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "jade sync");
+    for (int f = 0; f < F; ++f) {
+        lsvd_joint_trace t;
+        const bool trivial = n <= 1;
+        t.initial_offdiag = trivial ? 0.0 : h_init[f];
+        t.final_offdiag = trivial ? 0.0 : std::sqrt(h_off[f]);
+        t.sweeps = trivial ? 0 : h_sweeps[f];
+        t.rotations = h_rot[2 * size_t(f)];
+        t.rejected_rotations = h_rot[2 * size_t(f) + 1];
+        traces[f] = t;
+    }
+    return LSVD_OK;
+}
