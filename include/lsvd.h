@@ -216,6 +216,44 @@ LSVD_API lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, int6
                                        double* V, double* diag, lsvd_joint_trace* traces,
                                        uint32_t flags);
 
+/* ------------------------------------------------ large polar factor ---- */
+/* Polar factor Q (m x n, Q^T Q = I) of a large dense A (m >= n) by the
+ * Newton-Schulz iteration X <- X (3I - X^T X)/2 from X0 = A/||A||_F.
+ * Replaces newton_schulz_polar (src/lie_svd_small.rs:158-183) -- the
+ * reference applies it to square n <= 64 matrices inside LieSvdSmall::solve;
+ * this entry runs the same iteration and stopping rule on large m x n inputs:
+ *   LSVD_PREC_FP64       : FP64 GEMMs throughout, delta < 1e-13 sqrt(n) (cap 120);
+ *   LSVD_PREC_MIXED_TF32 : tcgen05 TF32 products (FP32 accumulation) until the
+ *   LSVD_PREC_MIXED_BF16   update reaches the low-precision floor, then FP64
+ *                          refinement iterations to delta < 1e-13 sqrt(n).
+ * The mixed precisions need m and n to be multiples of 128.  Singular values
+ * of A below ~u sigma_1 (u = 2^-11 TF32, 2^-8 BF16) are not resolved by the
+ * low-precision phase: the result is then orthogonal to working precision but
+ * differs from A's polar factor in that subspace.  Returns LSVD_NOT_CONVERGED
+ * (with Q written) when the cap is reached or the iteration diverged. */
+typedef struct lsvd_polar_info {
+    int32_t iters_lowp; /* TF32/BF16 iterations */
+    int32_t iters_fp64; /* FP64 iterations (refinement, or all for FP64) */
+    double orth;        /* ||Q^T Q - I||_F of the returned factor */
+    double flops_lowp;  /* 4 m n^2 per low-precision iteration */
+    double flops_fp64;  /* 4 m n^2 per FP64 iteration */
+    int32_t converged;
+    int32_t pad_;
+} lsvd_polar_info;
+
+LSVD_API lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, const double* A,
+                                    int64_t lda, double* Q, int64_t ldq, lsvd_precision precision,
+                                    lsvd_polar_info* info, uint32_t flags);
+
+/* C = A B^T (FP32, row-major M x N) with A (M x K), B (N x K) rounded to TF32
+ * or BF16 and multiplied on the tcgen05 tensor cores with FP32 accumulation:
+ * the product kernel of the mixed polar iteration, exposed for testing.
+ * Device pointers; M, N multiples of 128, K of 32 (TF32) or 64 (BF16).
+ * No counterpart in the reference. */
+LSVD_API lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N, int64_t K,
+                                       const float* A, const float* B, float* C,
+                                       lsvd_precision precision);
+
 /* ----------------------------------------------------- rotor schedule ---- */
 /* target: 0 = "mzi_mesh", 1 = "fpga_rotor_mesh" (HardwareTarget,
  * src/lie_svd_compiler.rs:12-25).  The JSON text (NUL-terminated) is written

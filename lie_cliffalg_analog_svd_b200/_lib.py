@@ -47,6 +47,12 @@ class JointTrace(C.Structure):
                 ("sweeps", C.c_int64), ("rotations", C.c_int64), ("rejected_rotations", C.c_int64)]
 
 
+class PolarInfo(C.Structure):
+    _fields_ = [("iters_lowp", C.c_int32), ("iters_fp64", C.c_int32), ("orth", C.c_double),
+                ("flops_lowp", C.c_double), ("flops_fp64", C.c_double), ("converged", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
 class LsvdError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"lsvd status {status}: {msg}")
@@ -78,6 +84,8 @@ SIGNATURES = {
     "lsvd_svd_batched_noalloc_f64": (C.c_int, [P, I64, P, P, P, P, P, P, U32]),
     "lsvd_joint_params_for_n": (JointParams, [I64]),
     "lsvd_jade_sym_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, U32]),
+    "lsvd_polar_f64": (C.c_int, [P, I64, I64, P, I64, P, I64, C.c_int, P, U32]),
+    "lsvd_gemm_nt_lowp": (C.c_int, [P, I64, I64, I64, P, P, P, C.c_int]),
     "lsvd_schedule_from_orthogonal": (C.c_int, [I64, P, C.c_int32, P, I64, C.POINTER(I64)]),
     "lsvd_schedule_from_rotors": (C.c_int, [P, I64, I64, C.c_int32, P, I64, C.POINTER(I64)]),
 }

@@ -396,3 +396,65 @@ class LieSvdJoint:
         traces = [JointDiagonalizationTrace(t.initial_offdiag, t.final_offdiag, t.sweeps,
                                             t.rotations, t.rejected_rotations) for t in tr]
         return v, d, traces
+
+
+class PolarResult:
+    """Polar factor with the iteration's diagnostics."""
+
+    def __init__(self, q, info: L.PolarInfo, status: int):
+        self.q = q
+        self.iters_lowp = int(info.iters_lowp)
+        self.iters_fp64 = int(info.iters_fp64)
+        self.orth = float(info.orth)
+        self.flops_lowp = float(info.flops_lowp)
+        self.flops_fp64 = float(info.flops_fp64)
+        self.converged = bool(info.converged)
+        self.status = status
+
+
+def polar(a, precision: str = "fp64", ctx: Context | None = None) -> PolarResult:
+    """Polar factor Q of a large m x n matrix (m >= n) by Newton-Schulz
+    (``newton_schulz_polar``, src/lie_svd_small.rs:158-183): FP64 throughout,
+    or TF32/BF16 tensor-core iterations followed by FP64 refinement.  ``a``:
+    numpy array (host path) or a contiguous float64 CUDA torch tensor (device
+    path, Q returned as a torch tensor)."""
+    ctx = ctx or default_context()
+    prec = PRECISIONS[precision]
+    info = L.PolarInfo()
+    is_torch = type(a).__module__.startswith("torch")
+    if is_torch:
+        import torch
+        assert a.is_cuda and a.dtype == torch.float64 and a.is_contiguous() and a.dim() == 2
+        m, n = a.shape
+        q = torch.empty_like(a)
+        st = ctx.lib.lsvd_polar_f64(ctx.handle, m, n, C.c_void_p(a.data_ptr()), n,
+                                    C.c_void_p(q.data_ptr()), n, prec, C.byref(info),
+                                    L.DEVICE_POINTERS)
+    else:
+        a = _f64(a)
+        m, n = a.shape
+        q = np.empty_like(a)
+        st = ctx.lib.lsvd_polar_f64(ctx.handle, m, n, _ptr(a), n, _ptr(q), n, prec,
+                                    C.byref(info), 0)
+    if st not in (L.OK, L.NOT_CONVERGED):
+        _check(ctx.lib, ctx.handle, st, "polar")
+    return PolarResult(q, info, st)
+
+
+def gemm_nt_lowp(a, b, precision: str = "tf32", ctx: Context | None = None):
+    """C = A B^T on the tcgen05 tensor cores with TF32 or BF16 operands and
+    FP32 accumulation (the product kernel of the mixed polar iteration).
+    ``a`` (M x K), ``b`` (N x K): contiguous float32 CUDA torch tensors."""
+    import torch
+    ctx = ctx or default_context()
+    assert a.is_cuda and b.is_cuda and a.dtype == torch.float32 and b.dtype == torch.float32
+    a = a.contiguous(); b = b.contiguous()
+    M, K = a.shape
+    N, K2 = b.shape
+    assert K == K2
+    c = torch.empty((M, N), dtype=torch.float32, device=a.device)
+    st = ctx.lib.lsvd_gemm_nt_lowp(ctx.handle, M, N, K, C.c_void_p(a.data_ptr()),
+                                   C.c_void_p(b.data_ptr()), C.c_void_p(c.data_ptr()),
+                                   PRECISIONS[precision])
+    _check(ctx.lib, ctx.handle, st, "gemm_nt_lowp")
+    return c

@@ -98,8 +98,9 @@ extern "C" lsvd_status lsvd_context_create(int device, lsvd_context** out) {
 lsvd_context::~lsvd_context() {
     cudaSetDevice(device);
     for (auto& kv : plans) kv.second.reset();
-    for (auto* b : {&ws_a, &ws_u, &ws_s, &ws_vt, &ws_diag, &ws_misc, &ws_rot})
+    for (auto* b : {&ws_a, &ws_u, &ws_s, &ws_vt, &ws_diag, &ws_misc, &ws_rot, &ws_polar})
         b->release();
+    lsvd_destroy_blas(cublas);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 

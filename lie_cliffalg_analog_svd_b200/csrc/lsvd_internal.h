@@ -85,7 +85,8 @@ struct lsvd_context {
     bool own_stream = false;
     std::string last_error;
     int64_t launches = 0;
-    DeviceBuffer ws_a, ws_u, ws_s, ws_vt, ws_diag, ws_misc, ws_rot;
+    DeviceBuffer ws_a, ws_u, ws_s, ws_vt, ws_diag, ws_misc, ws_rot, ws_polar;
+    void* cublas = nullptr;  // cublasHandle_t of the large-polar FP64 GEMMs, created on first use
     std::unordered_map<uint64_t, std::unique_ptr<BatchPlan>> plans;
     ~lsvd_context();
 };
@@ -105,6 +106,9 @@ lsvd_status lsvd_single_small(lsvd_context* ctx, int64_t n, const double* A, int
                               lsvd_diag* diag, lsvd_rotor* rotors, int64_t rotor_cap,
                               int64_t* rotor_count, int32_t* perm, uint32_t flags,
                               int extra_flags, bool host_meta);
+
+// lsvd_polar.cu
+void lsvd_destroy_blas(void* handle);
 
 // lsvd_autotune.cu
 void lsvd_autotune_shapes(lsvd_context* ctx, lsvd_precision prec, ClassShape* shapes);

@@ -1,0 +1,445 @@
+// lsvd_polar.cu -- Newton-Schulz polar factor of a large m x n matrix
+// (newton_schulz_polar, src/lie_svd_small.rs:158-183, generalised to m >= n)
+// in three precisions:
+//   FP64       : X <- 0.5 X (3I - X^T X) from X0 = A/||A||_F with FP64 GEMMs
+//                (cuBLAS DGEMM: plain library GEMMs) and the reference's
+//                stopping rule (delta < 1e-13 sqrt(n), cap 120);
+//   TF32, BF16 : the same iteration on tensor cores (lsvd_tcgemm.cuh,
+//                tcgen05, FP32 accumulation) until the update reaches the
+//                low-precision floor, then FP64 refinement iterations until
+//                delta < 1e-13 sqrt(n).
+// The refinement restores orthogonality to working precision, but it
+// converges to the polar factor of the low-precision iterate: rounding in the
+// TF32/BF16 products perturbs X at ~u_lo ||X|| in every direction, so the
+// mixed result differs from A's polar factor by about u_lo sqrt(n) in
+// Frobenius norm (u_lo = 2^-11 TF32, 2^-8 BF16), more where A's singular
+// values fall below ~u_lo sigma_1.  The FP64 path has no such floor.
+#include <cublas_v2.h>
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "lsvd.h"
+#include "lsvd_internal.h"
+#include "lsvd_tcgemm.cuh"
+
+namespace {
+
+using namespace lsvd::tc;
+
+__device__ __forceinline__ float round_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// Low-precision operand store: BF16 (2 bytes) or TF32-rounded FP32 (4 bytes).
+template <int PREC>
+__device__ __forceinline__ void store_lo(void* base, size_t idx, float v) {
+    if (PREC == kBF16)
+        reinterpret_cast<__nv_bfloat16*>(base)[idx] = __float2bfloat16_rn(v);
+    else
+        reinterpret_cast<float*>(base)[idx] = round_tf32(v);
+}
+
+// X (m x n, FP32) = A / ||A||_F; Xlo = lo(X); Xt = lo(X)^T (n x m).
+// Also: the NS update X <- 1.5 X - 0.5 Y when Y != nullptr, with the squared
+// update norm accumulated per block into part[b] and the squared norm of the
+// new X into part[nblocks + b].  32x32 tiles through shared memory make the
+// transposed store coalesced.
+template <int PREC>
+__global__ void ns_update_kernel(int m, int n, float* X, const float* Y, const double* A, int lda,
+                                 double inv_scale, void* Xlo, void* Xt, double* part) {
+    __shared__ float tile[32][33];
+    __shared__ double red[8], redx[8];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;  // bx: column, by: row
+    const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 32 x 8 threads
+    double d2 = 0.0, x2 = 0.0;
+    for (int r = ty; r < 32; r += 8) {
+        const int i = by + r, j = bx + tx;
+        const size_t e = size_t(i) * n + j;
+        float x;
+        if (Y) {
+            const float x0 = X[e];
+            x = 1.5f * x0 - 0.5f * Y[e];
+            d2 += double(x - x0) * double(x - x0);
+        } else {
+            x = float(A[size_t(i) * lda + j] * inv_scale);
+        }
+        X[e] = x;
+        x2 += double(x) * double(x);
+        store_lo<PREC>(Xlo, e, x);
+        tile[r][tx] = x;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int j = bx + r, i = by + tx;  // transposed: row j of X^T, column i
+        store_lo<PREC>(Xt, size_t(j) * m + i, tile[tx][r]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+        x2 += __shfl_xor_sync(0xffffffffu, x2, o);
+    }
+    if (tx == 0) {
+        red[ty] = d2;
+        redx[ty] = x2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0, sx = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            s += red[w];
+            sx += redx[w];
+        }
+        const int b = blockIdx.y * gridDim.x + blockIdx.x;
+        part[b] = s;
+        part[gridDim.x * gridDim.y + b] = sx;
+    }
+}
+
+template <int PREC>
+__global__ void to_lo_kernel(size_t count, const float* src, void* dst) {
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < count;
+         e += size_t(gridDim.x) * blockDim.x)
+        store_lo<PREC>(dst, e, src[e]);
+}
+
+__global__ void sum_kernel(int count, const double* part, double* out) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < count; i += 256) s += part[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+__global__ void frob2_kernel(int m, int n, const double* A, int lda, double* part) {
+    __shared__ double red[256];
+    double s = 0.0;
+    const size_t tot = size_t(m) * n;
+    for (size_t e = blockIdx.x * size_t(256) + threadIdx.x; e < tot; e += size_t(gridDim.x) * 256) {
+        const double v = A[(e / n) * lda + e % n];
+        s += v * v;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// FP64: X <- 1.5 X - 0.5 Y, squared update norm per block; or X = A/scale.
+__global__ void ns_update64_kernel(size_t count, double* X, const double* Y, double* part) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (size_t e = blockIdx.x * size_t(256) + threadIdx.x; e < count; e += size_t(gridDim.x) * 256) {
+        const double x0 = X[e];
+        const double x = 0.5 * (3.0 * x0 - Y[e]);
+        X[e] = x;
+        s += (x - x0) * (x - x0);
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void scale64_kernel(int m, int n, const double* A, int lda, double inv, double* X) {
+    const size_t tot = size_t(m) * n;
+    for (size_t e = blockIdx.x * size_t(256) + threadIdx.x; e < tot; e += size_t(gridDim.x) * 256)
+        X[e] = A[(e / n) * lda + e % n] * inv;
+}
+
+__global__ void widen_kernel(size_t count, const float* X32, double* X64) {
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < count;
+         e += size_t(gridDim.x) * blockDim.x)
+        X64[e] = double(X32[e]);
+}
+
+// ||T - I||_F^2 partials for the orthogonality check of the final iterate.
+__global__ void orth2_kernel(int n, const double* T, double* part) {
+    __shared__ double red[256];
+    double s = 0.0;
+    const size_t tot = size_t(n) * n;
+    for (size_t e = blockIdx.x * size_t(256) + threadIdx.x; e < tot; e += size_t(gridDim.x) * 256) {
+        const double d = T[e] - ((e / n) == (e % n) ? 1.0 : 0.0);
+        s += d * d;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point, so the
+// library does not link libcuda directly (it loads on hosts without a driver).
+typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                             const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                             CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                             CUtensorMapFloatOOBfill);
+
+EncodeFn encode_fn() {
+    static EncodeFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeFn>(p);
+    }();
+    return fn;
+}
+
+// 2-D K-major map: rows x cols (cols = K contiguous), box 128 rows x 128 bytes.
+bool make_map(CUtensorMap* map, int prec, const void* ptr, int rows, int cols) {
+    EncodeFn fn = encode_fn();
+    if (!fn) return false;
+    const int elem = prec == kBF16 ? 2 : 4;
+    cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
+    cuuint64_t strides[1] = {cuuint64_t(cols) * elem};
+    cuuint32_t box[2] = {cuuint32_t(kSliceBytes / elem), cuuint32_t(kTile)};
+    cuuint32_t es[2] = {1, 1};
+    return fn(map, prec == kBF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+              const_cast<void*>(ptr), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int PREC>
+cudaError_t launch_gemm(cudaStream_t st, const void* A, const void* B, float* C, int M, int N, int K,
+                        int* err) {
+    CUtensorMap ma, mb;
+    if (!make_map(&ma, PREC, A, M, K) || !make_map(&mb, PREC, B, N, K)) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kSmemBytes);
+    if (e != cudaSuccess) return e;
+    tc_gemm_kernel<PREC><<<dim3(N / kTile, M / kTile), 128, kSmemBytes, st>>>(ma, mb, C, N, K, err);
+    return cudaGetLastError();
+}
+
+cublasHandle_t blas(lsvd_context* ctx) {
+    if (!ctx->cublas) {
+        cublasHandle_t h;
+        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return nullptr;
+        ctx->cublas = h;
+    }
+    cublasHandle_t h = static_cast<cublasHandle_t>(ctx->cublas);
+    cublasSetStream(h, ctx->stream);
+    return h;
+}
+
+}  // namespace
+
+void lsvd_destroy_blas(void* h) {
+    if (h) cublasDestroy(static_cast<cublasHandle_t>(h));
+}
+
+extern "C" lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N, int64_t K,
+                                         const float* A, const float* B, float* C,
+                                         lsvd_precision precision) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    if (precision != LSVD_PREC_MIXED_TF32 && precision != LSVD_PREC_MIXED_BF16)
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_gemm_nt_lowp: precision must be TF32 or BF16");
+    const int prec = precision == LSVD_PREC_MIXED_BF16 ? kBF16 : kTF32;
+    const int kq = kSliceBytes / (prec == kBF16 ? 2 : 4);
+    if (M <= 0 || N <= 0 || K <= 0 || M % kTile || N % kTile || K % kq || M > (1 << 20) ||
+        N > (1 << 20) || K > (1 << 24))
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "lsvd_gemm_nt_lowp: M, N multiples of 128, K of the slice");
+    if (!A || !B || !C) return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "null pointer");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    cudaError_t e;
+    const size_t ea = size_t(M) * K, eb = size_t(N) * K;
+    const size_t esz = prec == kBF16 ? 2 : 4;
+    char* ws = static_cast<char*>(ctx->ws_a.get((ea + eb) * esz + 1024 + 16, &e));
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "gemm workspace");
+    void* alo = ws;
+    void* blo = ws + ((ea * esz + 255) & ~size_t(255));
+    int* err = reinterpret_cast<int*>(static_cast<char*>(ws) + ctx->ws_a.bytes - 16);
+    cudaMemsetAsync(err, 0, 4, st);
+    if (prec == kBF16) {
+        to_lo_kernel<kBF16><<<1024, 256, 0, st>>>(ea, A, alo);
+        to_lo_kernel<kBF16><<<1024, 256, 0, st>>>(eb, B, blo);
+        e = launch_gemm<kBF16>(st, alo, blo, C, int(M), int(N), int(K), err);
+    } else {
+        to_lo_kernel<kTF32><<<1024, 256, 0, st>>>(ea, A, alo);
+        to_lo_kernel<kTF32><<<1024, 256, 0, st>>>(eb, B, blo);
+        e = launch_gemm<kTF32>(st, alo, blo, C, int(M), int(N), int(K), err);
+    }
+    ctx->launches += 3;
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "tc gemm launch");
+    int herr = 0;
+    if ((e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "tc gemm sync");
+    if (herr) return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "tc gemm: pipeline wait timed out");
+    return LSVD_OK;
+}
+
+extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, const double* A,
+                                      int64_t lda, double* Q, int64_t ldq, lsvd_precision precision,
+                                      lsvd_polar_info* info, uint32_t flags) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    if (m <= 0 || n <= 0 || m < n) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "polar: need m >= n >= 1");
+    if (!A || !Q || lda < n || ldq < n) return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "polar: bad pointer");
+    const bool lowp = precision == LSVD_PREC_MIXED_TF32 || precision == LSVD_PREC_MIXED_BF16;
+    if (lowp && (m % kTile || n % kTile))
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "polar: TF32/BF16 need m, n multiples of 128");
+    if (m * n > (int64_t(1) << 31)) return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "polar: too large");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    cublasHandle_t h = blas(ctx);
+    if (!h) return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "cublasCreate failed");
+    const bool dev = (flags & LSVD_DEVICE_POINTERS) != 0;
+    const size_t mn = size_t(m) * n, nn = size_t(n) * n;
+    const int prec = precision == LSVD_PREC_MIXED_BF16 ? kBF16 : kTF32;
+    const size_t lo = prec == kBF16 ? 2 : 4;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    // workspace: A64 | X64 | Y64 | T64 | part | (X32 | Y32 | T32 | Xlo | Xt | Tlo | err)
+    const int nparts = 4096;
+    size_t bytes = al(mn * 8) * 3 + al(nn * 8) + al(nparts * 8) + 64;
+    if (lowp) bytes += al(mn * 4) * 2 + al(nn * 4) + al(mn * lo) * 2 + al(nn * lo) + 64;
+    cudaError_t e;
+    char* ws = static_cast<char*>(ctx->ws_polar.get(bytes, &e));
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar workspace");
+    char* p = ws;
+    double* A64 = reinterpret_cast<double*>(p); p += al(mn * 8);
+    double* X64 = reinterpret_cast<double*>(p); p += al(mn * 8);
+    double* Y64 = reinterpret_cast<double*>(p); p += al(mn * 8);
+    double* T64 = reinterpret_cast<double*>(p); p += al(nn * 8);
+    double* part = reinterpret_cast<double*>(p); p += al(nparts * 8);
+    double* dsum = reinterpret_cast<double*>(p); p += 64;
+    if ((e = cudaMemcpy2DAsync(A64, size_t(n) * 8, A, size_t(lda) * 8, size_t(n) * 8, size_t(m),
+                               cudaMemcpyDefault, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "polar copy A");
+    const double refn = std::sqrt(double(n));
+    auto read_sum = [&](int count, double* out) -> cudaError_t {
+        sum_kernel<<<1, 256, 0, st>>>(count, part, dsum);
+        cudaError_t ee = cudaMemcpyAsync(out, dsum, 8, cudaMemcpyDeviceToHost, st);
+        if (ee == cudaSuccess) ee = cudaStreamSynchronize(st);
+        return ee;
+    };
+    frob2_kernel<<<1024, 256, 0, st>>>(int(m), int(n), A64, int(n), part);
+    double f2 = 0.0;
+    if ((e = read_sum(1024, &f2)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar norm");
+    const double inv = 1.0 / std::max(std::sqrt(f2), 1e-300);
+    int it_lo = 0, it_hi = 0;
+    double flops_lo = 0.0, flops_hi = 0.0;
+    const double one = 1.0, zero = 0.0;
+    if (lowp) {
+        float* X32 = reinterpret_cast<float*>(p); p += al(mn * 4);
+        float* Y32 = reinterpret_cast<float*>(p); p += al(mn * 4);
+        float* T32 = reinterpret_cast<float*>(p); p += al(nn * 4);
+        void* Xlo = p; p += al(mn * lo);
+        void* Xt = p; p += al(mn * lo);
+        void* Tlo = p; p += al(nn * lo);
+        int* err = reinterpret_cast<int*>(p);
+        cudaMemsetAsync(err, 0, 4, st);
+        const dim3 ug(unsigned(n / 32), unsigned(m / 32));
+        const int nub = int(ug.x * ug.y);
+        double* upart = Y64;  // Y64 is unused in the low-precision phase: 2 partials per block
+        if (prec == kBF16)
+            ns_update_kernel<kBF16><<<ug, 256, 0, st>>>(int(m), int(n), X32, nullptr, A64, int(n), inv, Xlo, Xt, upart);
+        else
+            ns_update_kernel<kTF32><<<ug, 256, 0, st>>>(int(m), int(n), X32, nullptr, A64, int(n), inv, Xlo, Xt, upart);
+        // Stop the low-precision phase when the relative update
+        // delta/||X||_F reaches a few units of the low precision: beyond it
+        // the iterate only moves by rounding noise, and from there the FP64
+        // iteration is in its quadratic regime (e <- 1.5 e^2).
+        const double floor_rel = prec == kBF16 ? 8 * 3.90625e-3 : 8 * 4.8828125e-4;
+        for (int it = 0; it < 100; ++it) {
+            // T = X^T X = Xt Xt^T (n x n, K = m); Y = X T = Xlo T^T (m x n, K = n)
+            if (prec == kBF16) {
+                e = launch_gemm<kBF16>(st, Xt, Xt, T32, int(n), int(n), int(m), err);
+                if (e == cudaSuccess) to_lo_kernel<kBF16><<<1024, 256, 0, st>>>(nn, T32, Tlo);
+                if (e == cudaSuccess) e = launch_gemm<kBF16>(st, Xlo, Tlo, Y32, int(m), int(n), int(n), err);
+                if (e == cudaSuccess)
+                    ns_update_kernel<kBF16><<<ug, 256, 0, st>>>(int(m), int(n), X32, Y32, nullptr, 0, 0.0, Xlo, Xt, upart);
+            } else {
+                e = launch_gemm<kTF32>(st, Xt, Xt, T32, int(n), int(n), int(m), err);
+                if (e == cudaSuccess) to_lo_kernel<kTF32><<<1024, 256, 0, st>>>(nn, T32, Tlo);
+                if (e == cudaSuccess) e = launch_gemm<kTF32>(st, Xlo, Tlo, Y32, int(m), int(n), int(n), err);
+                if (e == cudaSuccess)
+                    ns_update_kernel<kTF32><<<ug, 256, 0, st>>>(int(m), int(n), X32, Y32, nullptr, 0, 0.0, Xlo, Xt, upart);
+            }
+            ctx->launches += 4;
+            if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar tc iteration");
+            sum_kernel<<<1, 256, 0, st>>>(nub, upart, dsum);
+            sum_kernel<<<1, 256, 0, st>>>(nub, upart + nub, dsum + 1);
+            double d2x2[2] = {0.0, 0.0};
+            int herr = 0;
+            if ((e = cudaMemcpyAsync(d2x2, dsum, 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(st)) != cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "polar tc sync");
+            if (herr) return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "tc gemm: pipeline wait timed out");
+            it_lo = it + 1;
+            flops_lo += 4.0 * double(m) * double(n) * double(n);
+            if (!std::isfinite(d2x2[0]) || !std::isfinite(d2x2[1])) break;
+            if (std::sqrt(d2x2[0]) < floor_rel * std::sqrt(d2x2[1])) break;
+        }
+        widen_kernel<<<2048, 256, 0, st>>>(mn, X32, X64);
+    } else {
+        scale64_kernel<<<2048, 256, 0, st>>>(int(m), int(n), A64, int(n), inv, X64);
+    }
+    // FP64 iterations (refinement, or the whole FP64 iteration): cuBLAS works
+    // column-major, so the row-major X (m x n) is the column-major X^T (n x m).
+    bool conv = false;
+    const int cap = lowp ? 120 - it_lo : 120;
+    for (int it = 0; it < cap; ++it) {
+        // T = X^T X  ->  col-major: X^T (n x m) * (X^T)^T
+        if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, int(n), int(n), int(m), &one, X64, int(n), X64,
+                        int(n), &zero, T64, int(n)) != CUBLAS_STATUS_SUCCESS ||
+            cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, int(n), int(m), int(n), &one, T64, int(n), X64,
+                        int(n), &zero, Y64, int(n)) != CUBLAS_STATUS_SUCCESS)
+            return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "cublasDgemm failed");
+        ns_update64_kernel<<<nparts, 256, 0, st>>>(mn, X64, Y64, part);
+        ctx->launches += 1;
+        double d2 = 0.0;
+        if ((e = read_sum(nparts, &d2)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar fp64 sync");
+        it_hi = it + 1;
+        flops_hi += 4.0 * double(m) * double(n) * double(n);
+        const double delta = std::sqrt(d2);
+        if (!std::isfinite(d2) || delta > 1e6 * refn) break;  // divergence (:169)
+        if (delta < 1e-13 * refn) {                            // POLAR_TOL (:173)
+            conv = true;
+            break;
+        }
+    }
+    // orthogonality of the returned factor: ||X^T X - I||_F
+    cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, int(n), int(n), int(m), &one, X64, int(n), X64, int(n), &zero,
+                T64, int(n));
+    orth2_kernel<<<nparts, 256, 0, st>>>(int(n), T64, part);
+    double o2 = 0.0;
+    if ((e = read_sum(nparts, &o2)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar orth");
+    if ((e = cudaMemcpy2DAsync(Q, size_t(ldq) * 8, X64, size_t(n) * 8, size_t(n) * 8, size_t(m),
+                               cudaMemcpyDefault, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "polar copy out");
+    if (info) {
+        info->iters_lowp = it_lo;
+        info->iters_fp64 = it_hi;
+        info->orth = std::sqrt(o2);
+        info->flops_lowp = flops_lo;
+        info->flops_fp64 = flops_hi;
+        info->converged = conv ? 1 : 0;
+        info->pad_ = 0;
+    }
+    return conv ? LSVD_OK : LSVD_NOT_CONVERGED;
+}

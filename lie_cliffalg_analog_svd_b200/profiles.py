@@ -189,13 +189,20 @@ def uneven_batch_workload(count: int, seed: int, n_lo: int = 2, n_hi: int = 64,
     return ns, a, sig
 
 
-def conditioned_matrix(m: int, n: int, kappa: float, seed: int):
-    """``Q1 diag(s) Q2^T`` with a geometric spectrum from 1 down to 1/kappa."""
+def conditioned_factors(m: int, n: int, kappa: float, seed: int):
+    """``(Q1, s, Q2)``: Q1 m x k and Q2 n x k with orthonormal columns
+    (k = min(m, n)), s geometric from 1 down to 1/kappa."""
     rng = np.random.default_rng(seed)
     k = min(m, n)
     s = kappa ** (-np.arange(k) / max(k - 1, 1))
     q1 = np.linalg.qr(rng.standard_normal((m, k)))[0]
     q2 = random_orthogonal(n, rng)[:, :k]
+    return q1, s, q2
+
+
+def conditioned_matrix(m: int, n: int, kappa: float, seed: int):
+    """``Q1 diag(s) Q2^T`` with a geometric spectrum from 1 down to 1/kappa."""
+    q1, s, q2 = conditioned_factors(m, n, kappa, seed)
     return (q1 * s[None, :]) @ q2.T, s
 
 
