@@ -1,7 +1,7 @@
 #!/usr/bin/env python
-"""Benchmark of the batched uneven SVD workload on B200.
+"""Benchmarks on B200.  The default workload is the batched uneven SVD.
 
-Workload (one "step"): 100,000 square f64 matrices, n ~ U{2..64},
+Default workload (one "step"): 100,000 square f64 matrices, n ~ U{2..64},
 A = Q1 diag(s) Q2^T with Haar Q1, Q2, s_i = 10^(-k i/(n-1)), k ~ U[0, 12],
 5% with a repeated-singular-value cluster (seeded synthetic data; the
 reference publishes no dataset).  Each matrix takes the exact route the
@@ -9,6 +9,16 @@ reference dispatcher takes for it: LieSvdMicro for n <= 4, LieSvdSmall
 otherwise (newton_schulz_polar + Jacobi eigensolve + U = QV + repair).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload batched|polar|jade|single] [--precision fp64|tf32|bf16]
+
+Other workloads (each prints its own JSON line):
+  polar  : Newton-Schulz polar factor of 16 dense matrices per step, 4096x4096
+           and 8192x2048 alternating, A = Q1 diag(s) Q2^T with geometric spectra
+           of condition 1e2, 1e5, 1e8 (metric: polar TFLOP/s);
+  jade   : Phase-JADE of 512 families of K=64 symmetric 256x256 matrices,
+           A_k = Q diag(d_k) Q^T + eps E_k, eps cycling over {0, 1e-8, 1e-4}
+           (metric: families/s);
+  single : one 64x64 Gaussian through the exact polar/Jacobi route (SVDs/s).
 
 Prints ONE JSON line (rank 0).  ``value`` is SVDs/s of the whole job with the
 inputs resident in HBM (CUDA events on the launching stream, max over ranks);
@@ -49,6 +59,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="batched", choices=["batched", "polar", "jade", "single"])
+    ap.add_argument("--families", type=int, default=512)
     return ap.parse_args()
 
 
@@ -371,11 +383,389 @@ def run_b200(args):
     return 0
 
 
+# ------------------------------------------------------- other workloads ----
+
+def _base_line(args, metric_unit, value, ms, ws, workload, config, dtype):
+    return {"metric": METRIC, "value": value, "unit": metric_unit, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic", "config": {"workload": workload, **config}}
+
+
+def _init_dist():
+    import torch
+    ws, rank, local = dist_setup()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    return torch, ws, rank, local, device
+
+
+def _max_over_ranks(torch, ws, device, x):
+    if ws == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+POLAR_SHAPES = [(4096, 4096), (8192, 2048)]
+POLAR_KAPPAS = [1e2, 1e5, 1e8]
+POLAR_COUNT = 16
+
+
+def polar_inputs(torch, device, seed):
+    """The six distinct polar inputs (2 shapes x 3 condition numbers), built
+    on the device from a seeded generator: A = Q1 diag(s) Q2^T with Q1, Q2 from
+    QR of Gaussians and s geometric from 1 to 1/kappa.  Returns
+    [(shape, kappa, A, exact polar factor Q1 Q2^T)]."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    out = []
+    for (m, n) in POLAR_SHAPES:
+        for kappa in POLAR_KAPPAS:
+            q1 = torch.linalg.qr(torch.randn(m, n, generator=g, device=device, dtype=torch.float64))[0]
+            q2 = torch.linalg.qr(torch.randn(n, n, generator=g, device=device, dtype=torch.float64))[0]
+            s = kappa ** (-torch.arange(n, device=device, dtype=torch.float64) / (n - 1))
+            a = ((q1 * s) @ q2.T).contiguous()
+            out.append(((m, n), kappa, a, (q1 @ q2.T).contiguous()))
+            del q1, q2
+    return out
+
+
+def run_polar(args):
+    torch, ws, rank, local, device = _init_dist()
+    from lie_cliffalg_analog_svd_b200 import Context, polar
+    ctx = Context(local)
+    stream = torch.cuda.Stream(device)
+    ctx.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        inputs = polar_inputs(torch, device, args.seed + rank)
+    torch.cuda.synchronize()
+    order = [inputs[(t % 2) * 3 + (t // 2) % 3] for t in range(POLAR_COUNT)]
+    # validation pass (untimed): accuracy per shape / kappa
+    acc = []
+    for (shape, kappa, a, qex) in inputs:
+        r = polar(a, args.precision, ctx=ctx)
+        acc.append({"shape": list(shape), "kappa": kappa, "iters_lowp": r.iters_lowp,
+                    "iters_fp64": r.iters_fp64, "orth": r.orth,
+                    "dist_to_exact_polar": float(torch.linalg.norm(r.q - qex).item()),
+                    "converged": r.converged})
+    fp64_peak = fp64_peak_tflops(torch, device)
+
+    def step():
+        fl, gms, gfl = 0.0, 0.0, 0.0
+        for (_, _, a, _) in order:
+            r = polar(a, args.precision, ctx=ctx)
+            fl += r.flops_lowp + r.flops_fp64
+            if args.precision == "fp64":
+                gms += r.gemm_ms_fp64; gfl += r.flops_fp64
+            else:
+                gms += r.gemm_ms_lowp; gfl += r.flops_lowp
+        return fl, gms, gfl
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    launches0 = ctx.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    flops = gemm_ms = gemm_flops = 0.0
+    with ClockSampler(local) as clk:
+        time.sleep(0.4)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            f, gm, gf = step()
+            flops += f; gemm_ms += gm; gemm_flops += gf
+        e1.record(stream)
+        torch.cuda.synchronize()
+        time.sleep(0.2)
+    ms = _max_over_ranks(torch, ws, device, e0.elapsed_time(e1) / args.steps)
+    launches = ctx.kernel_launches - launches0
+    value = ws * flops / args.steps / (ms * 1e-3) / 1e12
+    # e2e: host (pinned) A in, host Q out, through the C ABI
+    pinned = {}
+    for (shape, kappa, a, _) in inputs:
+        h = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        h.copy_(a)
+        pinned[id(a)] = (h.numpy(), torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy())
+    from lie_cliffalg_analog_svd_b200 import _lib as L
+    import ctypes as C
+    info = L.PolarInfo()
+    prec = {"fp64": 0, "tf32": 1, "bf16": 2}[args.precision]
+
+    def e2e_step():
+        for (_, _, a, _) in order:
+            ah, qh = pinned[id(a)]
+            m, n = ah.shape
+            st = ctx.lib.lsvd_polar_f64(ctx.handle, m, n, ah.ctypes.data, n, qh.ctypes.data, n, prec,
+                                        C.byref(info), 0)
+            assert st in (0, 1), st
+    e2e_step()
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    el = _max_over_ranks(torch, ws, device, (time.perf_counter() - t0) / args.steps)
+    bytes_io = sum(a.numel() * 8 for (_, _, a, _) in order)
+    peaks, peak_src = measured_peaks()
+    if args.precision == "fp64":
+        peak, psrc, kern = fp64_peak, "cuBLAS DGEMM 8192^3 measured in this run", "cuBLAS DGEMM (FP64 Newton-Schulz products)"
+    elif args.precision == "bf16":
+        peak, psrc, kern = peaks["bf16_tflops"], f"bf16_tflops ({peak_src})", "lsvd::tc::tc_gemm_kernel<BF16>"
+    else:
+        peak = peaks["bf16_tflops"] / 2
+        psrc, kern = f"bf16_tflops / 2 ({peak_src}; dense TF32 runs at half the BF16 rate)", "lsvd::tc::tc_gemm_kernel<TF32>"
+    achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
+    line = _base_line(args, "TFLOP/s", value, ms, ws, "polar_newton_schulz_16x(4096x4096|8192x2048)_kappa1e2-1e8",
+                      {"matrices_per_step": POLAR_COUNT, "shapes": POLAR_SHAPES, "kappas": POLAR_KAPPAS,
+                       "precision": args.precision,
+                       "flops_model": "4 m n^2 per executed Newton-Schulz iteration",
+                       "l2": "each input 134 MB, larger than the 126 MB L2",
+                       "parallelism": f"dp{ws} (independent matrices)"},
+                      "f64" if args.precision == "fp64" else f"{args.precision}+f64")
+    line.update({"polar_per_s": ws * POLAR_COUNT / (ms * 1e-3), "accuracy": acc,
+                 "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                              "frac": achieved / peak if achieved else None, "traffic": None,
+                              "kernel": kern, "peak_source": psrc,
+                              "timing": "summed CUDA-event durations of the GEMM launches on the polar stream"},
+                 "gpu_launches": launches, "clocks": clk.summary(),
+                 "e2e": {"value": ws * flops / args.steps / el / 1e12, "unit": "TFLOP/s",
+                         "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io,
+                         "ms_per_step": el * 1e3}})
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_polar(args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def cpu_baseline_polar(seconds: float):
+    """The oracle's newton_schulz_polar (src/lie_svd_small.rs:158-183, single
+    thread like the reference) on square matrices of growing size until the
+    time budget is spent; the rate is reported in TFLOP/s (4 n^3 per
+    iteration), so it compares with the GPU's per-flop rate."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # noqa: E402  (CPU baseline only)
+    from lie_cliffalg_analog_svd_b200 import profiles as P
+    fl, el, done = 0.0, 0.0, []
+    n = 128
+    while el < seconds and n <= 1024:
+        a, _ = P.conditioned_matrix(n, n, 1e5, seed=n)
+        t0 = time.perf_counter()
+        _, ok, it = O.ns_polar(a)
+        dt = time.perf_counter() - t0
+        fl += 4.0 * n ** 3 * it; el += dt; done.append(f"{n}^2 ({it} it, {dt:.1f} s)")
+        n *= 2
+    return {"value": fl / el / 1e12, "unit": "TFLOP/s", "cores": 1, "kind": "port",
+            "sample": "oracle newton_schulz_polar on kappa=1e5 matrices " + ", ".join(done)}
+
+
+def run_reference_polar(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline_polar(max(2.0, 60.0 / max(args.steps + args.warmup, 1)))
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = float(statistics.median(vals))
+    cb["value"] = v
+    line = _base_line(args, "TFLOP/s", v, None, args.gpus, "polar_newton_schulz (reference CPU, square proxies)",
+                      {"precision": "fp64", "l2": "n/a (CPU)"}, "f64")
+    line.update({"impl": "reference", "cpu_baseline": cb,
+                 "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+JADE_EPS = [0.0, 1e-8, 1e-4]
+
+
+def jade_inputs(torch, device, families, K, n, seed):
+    """Phase-JADE families on the device from a seeded generator:
+    A_k = Q diag(d_k) Q^T + eps E_k (Q from QR of a Gaussian, d_k ~ N(0,1),
+    E_k = (G + G^T)/2), eps cycling over {0, 1e-8, 1e-4} by family."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    m = torch.empty(families, K, n, n, dtype=torch.float64, device=device)
+    for f0 in range(0, families, 32):
+        f1 = min(families, f0 + 32)
+        q = torch.linalg.qr(torch.randn(f1 - f0, n, n, generator=g, device=device, dtype=torch.float64))[0]
+        d = torch.randn(f1 - f0, K, n, generator=g, device=device, dtype=torch.float64)
+        blk = (q[:, None] * d[:, :, None, :]) @ q.transpose(1, 2)[:, None]
+        eps = torch.tensor([JADE_EPS[f % 3] for f in range(f0, f1)], dtype=torch.float64, device=device)
+        e = torch.randn(f1 - f0, K, n, n, generator=g, device=device, dtype=torch.float64)
+        blk += eps[:, None, None, None] * 0.5 * (e + e.transpose(2, 3))
+        m[f0:f1] = blk
+        del q, d, blk, e
+    return m
+
+
+def run_jade(args):
+    torch, ws, rank, local, device = _init_dist()
+    import ctypes as C
+    from lie_cliffalg_analog_svd_b200 import Context
+    from lie_cliffalg_analog_svd_b200 import _lib as L
+    F, K, n = args.families, 64, 256
+    ctx = Context(local)
+    stream = torch.cuda.Stream(device)
+    ctx.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        m = jade_inputs(torch, device, F, K, n, args.seed + rank)
+        v = torch.empty(F, n, n, dtype=torch.float64, device=device)
+        d = torch.empty(F, K, n, dtype=torch.float64, device=device)
+    torch.cuda.synchronize()
+    traces = (L.JointTrace * F)()
+
+    def step():
+        st = ctx.lib.lsvd_jade_sym_f64(ctx.handle, F, K, n, C.c_void_p(m.data_ptr()), None,
+                                       C.c_void_p(v.data_ptr()), C.c_void_p(d.data_ptr()), traces,
+                                       L.DEVICE_POINTERS)
+        if st != 0:
+            raise L.LsvdError(st, ctx.lib.lsvd_context_last_error(ctx.handle).decode())
+
+    step()
+    sweeps = np.array([t.sweeps for t in traces]); rots = np.array([t.rotations for t in traces])
+    ratio = np.array([t.final_offdiag / max(t.initial_offdiag, 1e-300) for t in traces])
+    vv = v[:8]
+    orth = float(torch.linalg.norm(vv.transpose(1, 2) @ vv - torch.eye(n, device=device, dtype=torch.float64),
+                                   dim=(1, 2)).max().item())
+    acc = {"sweeps_mean": float(sweeps.mean()), "sweeps_max": int(sweeps.max()),
+           "rotations_mean": float(rots.mean()),
+           "final_over_initial_offdiag_by_eps": {str(e): float(ratio[[f for f in range(F) if JADE_EPS[f % 3] == e]].max())
+                                                 for e in JADE_EPS},
+           "orth_v_max_first8": orth}
+    for _ in range(args.warmup - 1):
+        step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    launches0 = ctx.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        time.sleep(0.4)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        time.sleep(0.2)
+    ms = _max_over_ranks(torch, ws, device, e0.elapsed_time(e1) / args.steps)
+    launches = ctx.kernel_launches - launches0
+    peaks, peak_src = measured_peaks()
+    # algorithmic bytes: every layer reads and writes each matrix of every
+    # live family once (rotations of block rows and columns), plus V
+    nb = n // 8
+    layers = nb - 1
+    bytes_step = float(sweeps.sum()) * layers * 2 * (K + 1) * n * n * 8
+    achieved = bytes_step / (ms * 1e-3) / 1e9
+    line = _base_line(args, "families/s", ws * F / (ms * 1e-3), ms, ws,
+                      f"phase_jade_{F}x(K=64,256x256)_eps(0,1e-8,1e-4)",
+                      {"families_per_gpu": F, "K": K, "n": n, "eps": JADE_EPS,
+                       "l2": "17 GB of matrices per step, larger than the 126 MB L2",
+                       "parallelism": f"dp{ws} (independent families)"}, "f64")
+    line.update({"accuracy": acc,
+                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                              "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                              "kernel": "jade_apply_kernel (+ jade_solve_kernel)",
+                              "peak_source": f"hbm_gbs ({peak_src})",
+                              "timing": "whole step (all JADE launches) on the launching stream"},
+                 "gpu_launches": launches, "clocks": clk.summary(), "e2e": None})
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_reference_jade(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # noqa: E402
+    from lie_cliffalg_analog_svd_b200 import profiles as P
+    fam = P.jade_family_workload(1, 64, 256, 1e-8, seed=args.seed)[0]
+    t0 = time.perf_counter()
+    O.LieSvdJoint.diagonalize_symmetric(list(fam))
+    el = time.perf_counter() - t0
+    v = 1.0 / el
+    line = _base_line(args, "families/s", v, el * 1e3, args.gpus, "phase_jade (reference CPU, 1 family K=64 256x256)",
+                      {"l2": "n/a (CPU)"}, "f64")
+    line.update({"impl": "reference",
+                 "cpu_baseline": {"value": v, "unit": "families/s", "cores": 1, "kind": "port",
+                                  "sample": f"1 family (K=64, n=256, eps=1e-8), {el:.1f} s, 1 thread"},
+                 "e2e": {"value": v, "unit": "families/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_single(args):
+    torch, ws, rank, local, device = _init_dist()
+    from lie_cliffalg_analog_svd_b200 import Context, LieSvdSmall
+    from lie_cliffalg_analog_svd_b200 import profiles as P
+    ctx = Context(local)
+    a = P.generate(64, "uniform_random", args.seed + rank)[0]
+    for _ in range(args.warmup):
+        LieSvdSmall.solve(a, ctx=ctx)
+    reps = 200
+    t0 = time.perf_counter()
+    for _ in range(reps * args.steps):
+        LieSvdSmall.solve(a, ctx=ctx)
+    el = _max_over_ranks(torch, ws, device, (time.perf_counter() - t0) / (reps * args.steps))
+    line = _base_line(args, "SVDs/s", ws / el, el * 1e3, ws, "single_64x64_gaussian_exact_route",
+                      {"n": 64, "calls_per_step": reps, "l2": "one 32 KB matrix (latency-bound)"}, "f64")
+    line.update({"e2e": {"value": ws / el, "unit": "SVDs/s", "h2d_bytes_per_step": 64 * 64 * 8,
+                         "d2h_bytes_per_step": 2 * 64 * 64 * 8 + 64 * 8, "ms_per_step": el * 1e3},
+                 "gpu_launches": None})
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_single(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # noqa: E402
+    from lie_cliffalg_analog_svd_b200 import profiles as P
+    a = P.generate(64, "uniform_random", args.seed)[0]
+    t0 = time.perf_counter(); k = 0
+    while time.perf_counter() - t0 < 5.0:
+        O.LieSvdSmall.solve(a); k += 1
+    el = (time.perf_counter() - t0) / k
+    line = _base_line(args, "SVDs/s", 1 / el, el * 1e3, args.gpus, "single_64x64_gaussian_exact_route (reference CPU)",
+                      {"n": 64, "l2": "n/a (CPU)"}, "f64")
+    line.update({"impl": "reference",
+                 "cpu_baseline": {"value": 1 / el, "unit": "SVDs/s", "cores": 1, "kind": "port",
+                                  "sample": f"{k} solves of one 64x64 Gaussian, 1 thread"},
+                 "e2e": {"value": 1 / el, "unit": "SVDs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
-        return run_reference(args)
-    return run_b200(args)
+        return {"batched": run_reference, "polar": run_reference_polar,
+                "jade": run_reference_jade, "single": run_reference_single}[args.workload](args)
+    return {"batched": run_b200, "polar": run_polar, "jade": run_jade,
+            "single": run_single}[args.workload](args)
 
 
 if __name__ == "__main__":

@@ -237,6 +237,8 @@ typedef struct lsvd_polar_info {
     double orth;        /* ||Q^T Q - I||_F of the returned factor */
     double flops_lowp;  /* 4 m n^2 per low-precision iteration */
     double flops_fp64;  /* 4 m n^2 per FP64 iteration */
+    double gemm_ms_lowp; /* summed CUDA-event durations of the TF32/BF16 GEMM launches */
+    double gemm_ms_fp64; /* ... and of the FP64 iteration GEMM launches */
     int32_t converged;
     int32_t pad_;
 } lsvd_polar_info;

@@ -49,7 +49,8 @@ class JointTrace(C.Structure):
 
 class PolarInfo(C.Structure):
     _fields_ = [("iters_lowp", C.c_int32), ("iters_fp64", C.c_int32), ("orth", C.c_double),
-                ("flops_lowp", C.c_double), ("flops_fp64", C.c_double), ("converged", C.c_int32),
+                ("flops_lowp", C.c_double), ("flops_fp64", C.c_double),
+                ("gemm_ms_lowp", C.c_double), ("gemm_ms_fp64", C.c_double), ("converged", C.c_int32),
                 ("pad_", C.c_int32)]
 
 

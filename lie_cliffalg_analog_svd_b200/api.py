@@ -408,6 +408,8 @@ class PolarResult:
         self.orth = float(info.orth)
         self.flops_lowp = float(info.flops_lowp)
         self.flops_fp64 = float(info.flops_fp64)
+        self.gemm_ms_lowp = float(info.gemm_ms_lowp)
+        self.gemm_ms_fp64 = float(info.gemm_ms_fp64)
         self.converged = bool(info.converged)
         self.status = status
 

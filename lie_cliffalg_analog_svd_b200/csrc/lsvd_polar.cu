@@ -244,6 +244,31 @@ cublasHandle_t blas(lsvd_context* ctx) {
     return h;
 }
 
+// Start/stop events around the GEMM launches of one iteration; the summed
+// durations are read after the iteration's own synchronisation.
+struct GemmTimer {
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    double ms = 0.0;
+    bool ok = true;
+    GemmTimer() {
+        for (auto& e : ev)
+            if (cudaEventCreate(&e) != cudaSuccess) ok = false;
+    }
+    ~GemmTimer() {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    void mark(int i, cudaStream_t st) {
+        if (ok) cudaEventRecord(ev[i], st);
+    }
+    void accumulate() {  // after the stream synchronised
+        float a = 0.f, b = 0.f;
+        if (ok && cudaEventElapsedTime(&a, ev[0], ev[1]) == cudaSuccess &&
+            cudaEventElapsedTime(&b, ev[2], ev[3]) == cudaSuccess)
+            ms += double(a) + double(b);
+    }
+};
+
 }  // namespace
 
 void lsvd_destroy_blas(void* h) {
@@ -341,6 +366,7 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
     const double inv = 1.0 / std::max(std::sqrt(f2), 1e-300);
     int it_lo = 0, it_hi = 0;
     double flops_lo = 0.0, flops_hi = 0.0;
+    GemmTimer tlo, thi;
     const double one = 1.0, zero = 0.0;
     if (lowp) {
         float* X32 = reinterpret_cast<float*>(p); p += al(mn * 4);
@@ -366,15 +392,23 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
         for (int it = 0; it < 100; ++it) {
             // T = X^T X = Xt Xt^T (n x n, K = m); Y = X T = Xlo T^T (m x n, K = n)
             if (prec == kBF16) {
+                tlo.mark(0, st);
                 e = launch_gemm<kBF16>(st, Xt, Xt, T32, int(n), int(n), int(m), err);
+                tlo.mark(1, st);
                 if (e == cudaSuccess) to_lo_kernel<kBF16><<<1024, 256, 0, st>>>(nn, T32, Tlo);
+                tlo.mark(2, st);
                 if (e == cudaSuccess) e = launch_gemm<kBF16>(st, Xlo, Tlo, Y32, int(m), int(n), int(n), err);
+                tlo.mark(3, st);
                 if (e == cudaSuccess)
                     ns_update_kernel<kBF16><<<ug, 256, 0, st>>>(int(m), int(n), X32, Y32, nullptr, 0, 0.0, Xlo, Xt, upart);
             } else {
+                tlo.mark(0, st);
                 e = launch_gemm<kTF32>(st, Xt, Xt, T32, int(n), int(n), int(m), err);
+                tlo.mark(1, st);
                 if (e == cudaSuccess) to_lo_kernel<kTF32><<<1024, 256, 0, st>>>(nn, T32, Tlo);
+                tlo.mark(2, st);
                 if (e == cudaSuccess) e = launch_gemm<kTF32>(st, Xlo, Tlo, Y32, int(m), int(n), int(n), err);
+                tlo.mark(3, st);
                 if (e == cudaSuccess)
                     ns_update_kernel<kTF32><<<ug, 256, 0, st>>>(int(m), int(n), X32, Y32, nullptr, 0, 0.0, Xlo, Xt, upart);
             }
@@ -389,6 +423,7 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
                 (e = cudaStreamSynchronize(st)) != cudaSuccess)
                 return lsvd_ctx_cuda(ctx, e, "polar tc sync");
             if (herr) return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "tc gemm: pipeline wait timed out");
+            tlo.accumulate();
             it_lo = it + 1;
             flops_lo += 4.0 * double(m) * double(n) * double(n);
             if (!std::isfinite(d2x2[0]) || !std::isfinite(d2x2[1])) break;
@@ -404,15 +439,20 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
     const int cap = lowp ? 120 - it_lo : 120;
     for (int it = 0; it < cap; ++it) {
         // T = X^T X  ->  col-major: X^T (n x m) * (X^T)^T
-        if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, int(n), int(n), int(m), &one, X64, int(n), X64,
-                        int(n), &zero, T64, int(n)) != CUBLAS_STATUS_SUCCESS ||
-            cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, int(n), int(m), int(n), &one, T64, int(n), X64,
-                        int(n), &zero, Y64, int(n)) != CUBLAS_STATUS_SUCCESS)
-            return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "cublasDgemm failed");
+        thi.mark(0, st);
+        const bool g1 = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, int(n), int(n), int(m), &one, X64, int(n),
+                                    X64, int(n), &zero, T64, int(n)) == CUBLAS_STATUS_SUCCESS;
+        thi.mark(1, st);
+        thi.mark(2, st);
+        const bool g2 = g1 && cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, int(n), int(m), int(n), &one, T64,
+                                          int(n), X64, int(n), &zero, Y64, int(n)) == CUBLAS_STATUS_SUCCESS;
+        thi.mark(3, st);
+        if (!g2) return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "cublasDgemm failed");
         ns_update64_kernel<<<nparts, 256, 0, st>>>(mn, X64, Y64, part);
         ctx->launches += 1;
         double d2 = 0.0;
         if ((e = read_sum(nparts, &d2)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar fp64 sync");
+        thi.accumulate();
         it_hi = it + 1;
         flops_hi += 4.0 * double(m) * double(n) * double(n);
         const double delta = std::sqrt(d2);
@@ -438,6 +478,8 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
         info->orth = std::sqrt(o2);
         info->flops_lowp = flops_lo;
         info->flops_fp64 = flops_hi;
+        info->gemm_ms_lowp = tlo.ms;
+        info->gemm_ms_fp64 = thi.ms;
         info->converged = conv ? 1 : 0;
         info->pad_ = 0;
     }

@@ -62,6 +62,7 @@ def test_status_strings_and_version(lib):
 def test_structs_match_header(lib):
     assert C.sizeof(L.Diag) == 48
     assert C.sizeof(L.Rotor) == 16
+    assert C.sizeof(L.PolarInfo) == 56
     assert np.dtype(L.DIAG_DTYPE).itemsize == 48
     assert np.dtype(L.ROTOR_DTYPE).itemsize == 16
 
