@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="batched", choices=["batched", "polar", "jade", "single"])
     ap.add_argument("--families", type=int, default=512)
+    ap.add_argument("--polar-size", default="full", choices=["full", "small"],
+                    help="small: 2048x2048 and 4096x1024 instead of 4096x4096 and 8192x2048")
     return ap.parse_args()
 
 
@@ -418,7 +420,7 @@ POLAR_KAPPAS = [1e2, 1e5, 1e8]
 POLAR_COUNT = 16
 
 
-def polar_inputs(torch, device, seed):
+def polar_inputs(torch, device, seed, shapes=POLAR_SHAPES):
     """The six distinct polar inputs (2 shapes x 3 condition numbers), built
     on the device from a seeded generator: A = Q1 diag(s) Q2^T with Q1, Q2 from
     QR of Gaussians and s geometric from 1 to 1/kappa.  Returns
@@ -426,7 +428,7 @@ def polar_inputs(torch, device, seed):
     g = torch.Generator(device=device)
     g.manual_seed(seed)
     out = []
-    for (m, n) in POLAR_SHAPES:
+    for (m, n) in shapes:
         for kappa in POLAR_KAPPAS:
             q1 = torch.linalg.qr(torch.randn(m, n, generator=g, device=device, dtype=torch.float64))[0]
             q2 = torch.linalg.qr(torch.randn(n, n, generator=g, device=device, dtype=torch.float64))[0]
@@ -443,8 +445,9 @@ def run_polar(args):
     ctx = Context(local)
     stream = torch.cuda.Stream(device)
     ctx.set_stream(stream.cuda_stream)
+    shapes = POLAR_SHAPES if args.polar_size == "full" else [(2048, 2048), (4096, 1024)]
     with torch.cuda.stream(stream):
-        inputs = polar_inputs(torch, device, args.seed + rank)
+        inputs = polar_inputs(torch, device, args.seed + rank, shapes)
     torch.cuda.synchronize()
     order = [inputs[(t % 2) * 3 + (t // 2) % 3] for t in range(POLAR_COUNT)]
     # validation pass (untimed): accuracy per shape / kappa
@@ -525,11 +528,13 @@ def run_polar(args):
         peak = peaks["bf16_tflops"] / 2
         psrc, kern = f"bf16_tflops / 2 ({peak_src}; dense TF32 runs at half the BF16 rate)", "lsvd::tc::tc_gemm_kernel<TF32>"
     achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
-    line = _base_line(args, "TFLOP/s", value, ms, ws, "polar_newton_schulz_16x(4096x4096|8192x2048)_kappa1e2-1e8",
-                      {"matrices_per_step": POLAR_COUNT, "shapes": POLAR_SHAPES, "kappas": POLAR_KAPPAS,
+    wl = "|".join(f"{m}x{n}" for m, n in shapes)
+    line = _base_line(args, "TFLOP/s", value, ms, ws, f"polar_newton_schulz_16x({wl})_kappa1e2-1e8",
+                      {"matrices_per_step": POLAR_COUNT, "shapes": shapes, "kappas": POLAR_KAPPAS,
                        "precision": args.precision,
                        "flops_model": "4 m n^2 per executed Newton-Schulz iteration",
-                       "l2": "each input 134 MB, larger than the 126 MB L2",
+                       "l2": "inputs of 134 MB (full) / 34 MB (small) each, 6 distinct per step, "
+                             "together larger than the 126 MB L2",
                        "parallelism": f"dp{ws} (independent matrices)"},
                       "f64" if args.precision == "fp64" else f"{args.precision}+f64")
     line.update({"polar_per_s": ws * POLAR_COUNT / (ms * 1e-3), "accuracy": acc,
