@@ -18,7 +18,10 @@ Other workloads (each prints its own JSON line):
   jade   : Phase-JADE of 512 families of K=64 symmetric 256x256 matrices,
            A_k = Q diag(d_k) Q^T + eps E_k, eps cycling over {0, 1e-8, 1e-4}
            (metric: families/s);
-  single : one 64x64 Gaussian through the exact polar/Jacobi route (SVDs/s).
+  single : one 64x64 Gaussian through the exact polar/Jacobi route (SVDs/s);
+  adjoint: SVD/polar vector-Jacobian products of 4,096 matrices 128x64 (sigma
+           uniform in [0.1, 10], gap >= 1e-3, 10% with one 1e-6 gap) from the
+           stored rotor streams, cotangents N(0,1) on U, S, V and U V^T (VJPs/s).
 
 Prints ONE JSON line (rank 0).  ``value`` is SVDs/s of the whole job with the
 inputs resident in HBM (CUDA events on the launching stream, max over ranks);
@@ -59,7 +62,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="batched", choices=["batched", "polar", "jade", "single"])
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "polar", "jade", "single", "adjoint"])
     ap.add_argument("--families", type=int, default=512)
     ap.add_argument("--polar-size", default="full", choices=["full", "small"],
                     help="small: 2048x2048 and 4096x1024 instead of 4096x4096 and 8192x2048")
@@ -764,13 +768,203 @@ def run_reference_single(args):
     return 0
 
 
+ADJ_COUNT, ADJ_M, ADJ_N = 4096, 128, 64
+
+
+def numpy_svd_adjoint(u, s, v, ub, sb, vb, qb, gap_tol=0.0):
+    """The analytic thin-SVD + polar adjoint in numpy (the CPU comparison)."""
+    den = s[None, :] ** 2 - s[:, None] ** 2
+    close = np.abs(s[None, :] - s[:, None]) <= gap_tol * s.max()
+    f = np.where((den == 0) | close, 0.0, 1.0 / np.where(den == 0, 1.0, den))
+    np.fill_diagonal(f, 0.0)
+    g = u.T @ ub
+    h = v.T @ vb
+    mm = u.T @ qb @ v
+    core = (f * (g - g.T)) * s[None, :] + s[:, None] * (f * (h - h.T)) \
+        + (mm - mm.T) / (s[:, None] + s[None, :]) + np.diag(sb)
+    proj = (ub + qb @ v) - u @ (u.T @ (ub + qb @ v))
+    return u @ core @ v.T + (proj / s[None, :]) @ v.T
+
+
+def vjp_flops(m, n, rotations):
+    """FP64 flops of one adjoint: A^T Ubar, A^T Qbar and the three m x n
+    products of Abar (10 m n^2), seven n x n products (14 n^3), and the
+    replay (6 n flops per rotation)."""
+    return 10.0 * m * n * n + 14.0 * n ** 3 + 6.0 * n * rotations
+
+
+def run_adjoint(args):
+    torch, ws, rank, local, device = _init_dist()
+    from lie_cliffalg_analog_svd_b200 import Context, svd_batched_stream, svd_vjp
+    from lie_cliffalg_analog_svd_b200 import profiles as P
+    cnt, m, n = ADJ_COUNT, ADJ_M, ADJ_N
+    ctx = Context(local)
+    stream = torch.cuda.Stream(device)
+    ctx.set_stream(stream.cuda_stream)
+    a, sig = P.adjoint_workload(cnt, m, n, seed=args.seed + rank)
+    rng = np.random.default_rng(args.seed + 1 + rank)
+    cot = {k: rng.standard_normal(shape) for k, shape in
+           (("ub", (cnt, m, n)), ("sb", (cnt, n)), ("vb", (cnt, n, n)), ("qb", (cnt, m, n)))}
+    ad = torch.from_numpy(a).to(device)
+    cd = {k: torch.from_numpy(v).to(device) for k, v in cot.items()}
+    torch.cuda.synchronize()
+    # forward with the stream (and U, V for the accuracy check and the stored-V path)
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fwd = svd_batched_stream(ad, ctx=ctx)
+    e1.record(stream); torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    fwd_uv = svd_batched_stream(ad, want_uv=True, ctx=ctx)
+    counts = fwd.counts.cpu().numpy()
+    stream_bytes = fwd.stream_bytes()
+    uv_bytes = fwd.uv_bytes()
+    flops = float(sum(vjp_flops(m, n, int(c)) for c in counts))
+
+    def step(stored=False):
+        return svd_vjp(fwd, ubar=cd["ub"], sbar=cd["sb"], vbar=cd["vb"], qbar=cd["qb"], ctx=ctx,
+                       stored_vt=fwd_uv.vt if stored else None)
+
+    ab = step()
+    # accuracy on a subset: the analytic formula on the forward's own U, V
+    ab_h = ab[:32].cpu().numpy()
+    u_h = fwd_uv.u[:32].cpu().numpy(); vt_h = fwd_uv.vt[:32].cpu().numpy(); s_h = fwd_uv.s[:32].cpu().numpy()
+    gaps = np.min(-np.diff(sig, axis=1), axis=1)
+    errs = []
+    for t in range(32):
+        if gaps[t] < 1e-4:
+            continue
+        ref = numpy_svd_adjoint(u_h[t], s_h[t], vt_h[t].T, cot["ub"][t], cot["sb"][t], cot["vb"][t], cot["qb"][t])
+        errs.append(float(np.linalg.norm(ab_h[t] - ref) / np.linalg.norm(ref)))
+    fwd_sig_err = float(np.max(np.abs(fwd.s.cpu().numpy() - sig) / sig[:, :1]))
+    fp64_peak = fp64_peak_tflops(torch, device)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        l0 = ctx.kernel_launches
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return _max_over_ranks(torch, ws, device, e0.elapsed_time(e1) / args.steps), ctx.kernel_launches - l0
+
+    with ClockSampler(local) as clk:
+        time.sleep(0.4)
+        ms, launches = timed(step)
+        time.sleep(0.2)
+    ms_stored, _ = timed(lambda: step(True))
+    # e2e: host arrays through the C ABI (A, S, perm, stream, cotangents in; Abar out)
+    fwd_h = svd_batched_stream(a, ctx=ctx)
+
+    def e2e_step():
+        return svd_vjp(fwd_h, ubar=cot["ub"], sbar=cot["sb"], vbar=cot["vb"], qbar=cot["qb"], ctx=ctx)
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    el = _max_over_ranks(torch, ws, device, (time.perf_counter() - t0) / args.steps)
+    h2d = a.nbytes + sum(v.nbytes for v in cot.values()) + fwd_h.s.nbytes + fwd_h.perm.nbytes \
+        + fwd_h.rotors.nbytes + fwd_h.counts.nbytes
+    achieved = flops / (ms * 1e-3) / 1e12
+    line = _base_line(args, "VJPs/s", ws * cnt / (ms * 1e-3), ms, ws,
+                      f"svd_polar_vjp_rotor_replay_{cnt}x{m}x{n}",
+                      {"count_per_gpu": cnt, "m": m, "n": n, "sigma": "U[0.1, 10], gap >= 1e-3, 10% one 1e-6 gap",
+                       "cotangents": "N(0,1) on U, S, V and the polar factor",
+                       "l2": "A and cotangents 0.8 GB + streams per step, larger than the 126 MB L2",
+                       "parallelism": f"dp{ws} (independent matrices)"}, "f64")
+    line.update({
+        "accuracy": {"vs_analytic_fp64_rel_max": max(errs) if errs else None, "checked": len(errs),
+                     "forward_sigma_err_max": fwd_sig_err},
+        "memory": {"stream_bytes": stream_bytes, "stored_uv_bytes": uv_bytes,
+                   "rotations_mean": float(counts.mean()), "ratio_stream_over_uv": stream_bytes / uv_bytes},
+        "time": {"vjp_replay_ms": ms, "vjp_stored_v_ms": ms_stored, "forward_stream_ms": fwd_ms},
+        "roofline": {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": fp64_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+                     "kernel": "svd_vjp_kernel", "flops_per_launch": flops,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"},
+        "gpu_launches": launches, "clocks": clk.summary(),
+        "e2e": {"value": ws * cnt / el, "unit": "VJPs/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(a.nbytes), "ms_per_step": el * 1e3}})
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_adjoint(a[:256], {k: v[:256] for k, v in cot.items()},
+                                                    args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def cpu_baseline_adjoint(a, cot, seconds):
+    """Per matrix on the host cores: the oracle's solve_rectangular (the
+    reference's forward) and the analytic adjoint in numpy."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # noqa: E402  (CPU baseline only)
+    from concurrent.futures import ThreadPoolExecutor
+    cores = cpu_cores()
+    stop = time.perf_counter() + seconds
+    done = [0]
+    lock = threading.Lock()
+
+    def work(idx):
+        c = 0
+        while time.perf_counter() < stop:  # passes over the sample until the budget is spent
+            for t in idx:
+                if time.perf_counter() > stop:
+                    break
+                u, s, vt = O.LieSvdSmall.solve_rectangular(a[t])
+                numpy_svd_adjoint(u, s, vt.T, cot["ub"][t], cot["sb"][t], cot["vb"][t], cot["qb"][t])
+                c += 1
+        with lock:
+            done[0] += c
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        list(ex.map(work, np.array_split(np.arange(a.shape[0]), cores)))
+    el = time.perf_counter() - t0
+    return {"value": done[0] / el, "unit": "VJPs/s", "cores": cores, "kind": "port",
+            "sample": f"{done[0]} solves (passes over {a.shape[0]} of the 128x64 matrices): oracle "
+                      f"solve_rectangular + numpy analytic adjoint, {el:.1f} s on {cores} host threads"}
+
+
+def run_reference_adjoint(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    from lie_cliffalg_analog_svd_b200 import profiles as P
+    a, _ = P.adjoint_workload(256, ADJ_M, ADJ_N, seed=args.seed)
+    rng = np.random.default_rng(args.seed + 1)
+    cot = {"ub": rng.standard_normal(a.shape), "sb": rng.standard_normal((256, ADJ_N)),
+           "vb": rng.standard_normal((256, ADJ_N, ADJ_N)), "qb": rng.standard_normal(a.shape)}
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline_adjoint(a, cot, max(2.0, 60.0 / max(args.steps + args.warmup, 1)))
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = float(statistics.median(vals))
+    cb["value"] = v
+    line = _base_line(args, "VJPs/s", v, ADJ_COUNT / v * 1e3, args.gpus,
+                      f"svd_polar_vjp (reference CPU forward + numpy adjoint) {ADJ_M}x{ADJ_N}",
+                      {"l2": "n/a (CPU)"}, "f64")
+    line.update({"impl": "reference", "cpu_baseline": cb,
+                 "e2e": {"value": v, "unit": "VJPs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return {"batched": run_reference, "polar": run_reference_polar,
-                "jade": run_reference_jade, "single": run_reference_single}[args.workload](args)
+                "jade": run_reference_jade, "single": run_reference_single,
+                "adjoint": run_reference_adjoint}[args.workload](args)
     return {"batched": run_b200, "polar": run_polar, "jade": run_jade,
-            "single": run_single}[args.workload](args)
+            "single": run_single, "adjoint": run_adjoint}[args.workload](args)
 
 
 if __name__ == "__main__":

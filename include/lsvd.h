@@ -256,6 +256,44 @@ LSVD_API lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N, 
                                        const float* A, const float* B, float* C,
                                        lsvd_precision precision);
 
+/* ------------------------------------------- rotor stream and adjoint ---- */
+/* Batched thin SVD of `count` matrices of one shape m x n (m >= n, n <= 64,
+ * m <= 4096; packed row-major), keeping each matrix's accepted rotor stream
+ * and sort permutation so that U and V need not be stored.  Tall inputs go
+ * through qr_reduce (src/lie_svd_small.rs:373-418) and the square solve of R,
+ * square ones through the solve directly -- LieSvdSmall::solve
+ * (src/lie_svd_small.rs:296-336) for every n (no LieSvdMicro route here).
+ * Matrix t's stream is rotors[t*rotor_cap ..][0 .. rotor_count[t]); with
+ * perm[t*n ..] it gives V = G_1 G_2 ... G_k P (G_r rotates columns i, j by
+ * theta: v_i <- c v_i - s v_j, v_j <- s v_i + c v_j; P[:, j] = e_perm[j]).
+ * U (m x n) and Vt (n x n) may be NULL.  A stream longer than rotor_cap
+ * returns LSVD_ROTOR_OVERFLOW.  Host or device pointers (LSVD_DEVICE_POINTERS);
+ * synchronous.  No counterpart in the reference. */
+LSVD_API lsvd_status lsvd_svd_batched_stream_f64(lsvd_context* ctx, int64_t count, int64_t m, int64_t n,
+                                                 const double* A, double* U, double* S, double* Vt,
+                                                 lsvd_rotor* rotors, int64_t rotor_cap,
+                                                 int64_t* rotor_count, int32_t* perm, lsvd_diag* diags,
+                                                 uint32_t flags);
+
+/* Vector-Jacobian product of the thin SVD A = U diag(S) V^T and of its polar
+ * factor Q = U V^T: given the forward's A, S, perm and rotor stream (as
+ * written by lsvd_svd_batched_stream_f64) and cotangents Ubar (m x n), Sbar
+ * (n), Vbar (n x n, of V -- not of Vt) and Qbar (m x n), each may be NULL,
+ * writes Abar (m x n) for every matrix.  V is rebuilt by replaying the stream
+ * in reverse and U = A V S^-1 is recomputed; nothing of U or V is stored.
+ * The analytic thin-SVD adjoint with F_ij = 1/(s_j^2 - s_i^2) is used; F_ij
+ * is taken as 0 where |s_i - s_j| <= gap_tol * max(S) (gap_tol = 0: exact
+ * formula).  Needs S > 0 (else LSVD_BAD_ARGUMENT and that Abar zeroed).
+ * Vt (n x n per matrix) may be NULL; when given, V is read from it instead of
+ * replayed (the path that keeps V, for comparison; perm/rotors then unused).
+ * Host or device pointers; synchronous.  No counterpart in the reference. */
+LSVD_API lsvd_status lsvd_svd_vjp_f64(lsvd_context* ctx, int64_t count, int64_t m, int64_t n,
+                                      const double* A, const double* S, const int32_t* perm,
+                                      const lsvd_rotor* rotors, int64_t rotor_cap,
+                                      const int64_t* rotor_count, const double* Ubar,
+                                      const double* Sbar, const double* Vbar, const double* Qbar,
+                                      const double* Vt, double gap_tol, double* Abar, uint32_t flags);
+
 /* ----------------------------------------------------- rotor schedule ---- */
 /* target: 0 = "mzi_mesh", 1 = "fpga_rotor_mesh" (HardwareTarget,
  * src/lie_svd_compiler.rs:12-25).  The JSON text (NUL-terminated) is written

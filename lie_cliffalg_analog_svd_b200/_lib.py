@@ -87,6 +87,9 @@ SIGNATURES = {
     "lsvd_jade_sym_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, U32]),
     "lsvd_polar_f64": (C.c_int, [P, I64, I64, P, I64, P, I64, C.c_int, P, U32]),
     "lsvd_gemm_nt_lowp": (C.c_int, [P, I64, I64, I64, P, P, P, C.c_int]),
+    "lsvd_svd_batched_stream_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, I64, P, P, P, U32]),
+    "lsvd_svd_vjp_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, I64, P, P, P, P, P, P,
+                                   C.c_double, P, U32]),
     "lsvd_schedule_from_orthogonal": (C.c_int, [I64, P, C.c_int32, P, I64, C.POINTER(I64)]),
     "lsvd_schedule_from_rotors": (C.c_int, [P, I64, I64, C.c_int32, P, I64, C.POINTER(I64)]),
 }

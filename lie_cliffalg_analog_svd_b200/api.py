@@ -460,3 +460,105 @@ def gemm_nt_lowp(a, b, precision: str = "tf32", ctx: Context | None = None):
                                    PRECISIONS[precision])
     _check(ctx.lib, ctx.handle, st, "gemm_nt_lowp")
     return c
+
+
+class SvdStream:
+    """Forward of the stream-keeping batched SVD: sigma, sort permutation and
+    accepted rotor stream per matrix (U, Vt when requested)."""
+
+    def __init__(self, m, n, a, s, perm, rotors, counts, u, vt, diags, status, cap):
+        self.m, self.n = m, n
+        self.a = a
+        self.s = s
+        self.perm = perm
+        self.rotors = rotors
+        self.counts = counts
+        self.u = u
+        self.vt = vt
+        self.diags = diags
+        self.status = status
+        self.rotor_cap = cap
+
+    def stream_bytes(self) -> int:
+        """Bytes the adjoint needs beyond A: sigma, perm and the streams."""
+        nel = lambda x: int(x.numel()) if hasattr(x, "numel") else int(x.size)  # noqa: E731
+        return int(self.counts.sum()) * 16 + nel(self.s) * 8 + nel(self.perm) * 4
+
+    def uv_bytes(self) -> int:
+        """Bytes of the U and V intermediates this replaces."""
+        cnt = self.s.shape[0]
+        return cnt * (self.m * self.n + self.n * self.n) * 8
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def svd_batched_stream(a, rotor_cap: int | None = None, want_uv: bool = False,
+                       want_diag: bool = False, ctx: Context | None = None) -> SvdStream:
+    """Thin SVD of ``a`` (count, m, n), m >= n, n <= 64, keeping each matrix's
+    rotor stream (numpy host arrays, or a contiguous float64 CUDA torch tensor
+    for the device path, whose outputs are then torch tensors)."""
+    ctx = ctx or default_context()
+    cnt, m, n = a.shape
+    # default: room for 20 full sweeps of n (n - 1) / 2 rotations
+    cap = rotor_cap if rotor_cap is not None else 20 * (n * (n - 1) // 2) + 1
+    flags = L.WANT_DIAG if want_diag else 0
+    if _is_torch(a):
+        import torch
+        assert a.is_cuda and a.dtype == torch.float64 and a.is_contiguous()
+        dv = a.device
+        s = torch.empty((cnt, n), dtype=torch.float64, device=dv)
+        perm = torch.empty((cnt, n), dtype=torch.int32, device=dv)
+        rot = torch.empty((cnt, max(cap, 1), 16), dtype=torch.uint8, device=dv)
+        counts = torch.empty(cnt, dtype=torch.int64, device=dv)
+        u = torch.empty((cnt, m, n), dtype=torch.float64, device=dv) if want_uv else None
+        vt = torch.empty((cnt, n, n), dtype=torch.float64, device=dv) if want_uv else None
+        dg = torch.empty((cnt, C.sizeof(L.Diag)), dtype=torch.uint8, device=dv) if want_diag else None
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+        st = ctx.lib.lsvd_svd_batched_stream_f64(ctx.handle, cnt, m, n, ptr(a), ptr(u), ptr(s), ptr(vt),
+                                                 ptr(rot), cap, ptr(counts), ptr(perm), ptr(dg),
+                                                 flags | L.DEVICE_POINTERS)
+    else:
+        a = _f64(a)
+        s = np.empty((cnt, n)); perm = np.empty((cnt, n), dtype=np.int32)
+        rot = np.empty((cnt, max(cap, 1)), dtype=L.ROTOR_DTYPE)
+        counts = np.empty(cnt, dtype=np.int64)
+        u = np.empty((cnt, m, n)) if want_uv else None
+        vt = np.empty((cnt, n, n)) if want_uv else None
+        dg = np.empty(cnt, dtype=L.DIAG_DTYPE) if want_diag else None
+        p = lambda x: _ptr(x) if x is not None else None  # noqa: E731
+        st = ctx.lib.lsvd_svd_batched_stream_f64(ctx.handle, cnt, m, n, _ptr(a), p(u), _ptr(s), p(vt),
+                                                 _ptr(rot), cap, _ptr(counts), _ptr(perm), p(dg), flags)
+    if st not in (L.OK, L.NOT_CONVERGED, L.NONFINITE_INPUT):
+        _check(ctx.lib, ctx.handle, st, "svd_batched_stream")
+    return SvdStream(m, n, a, s, perm, rot, counts, u, vt, dg, st, cap)
+
+
+def svd_vjp(fwd: SvdStream, ubar=None, sbar=None, vbar=None, qbar=None, gap_tol: float = 0.0,
+            ctx: Context | None = None, stored_vt=None):
+    """Abar for cotangents on U (count, m, n), sigma (count, n), V (count, n, n)
+    and the polar factor U V^T (count, m, n), from the forward's rotor stream
+    (host numpy or device torch, matching the forward).  ``stored_vt``: read V
+    from it instead of replaying the stream (the comparison path)."""
+    ctx = ctx or default_context()
+    cnt, m, n = fwd.a.shape
+    if _is_torch(fwd.a):
+        import torch
+        ab = torch.empty_like(fwd.a)
+        ptr = lambda t: C.c_void_p(t.contiguous().data_ptr()) if t is not None else None  # noqa: E731
+        st = ctx.lib.lsvd_svd_vjp_f64(ctx.handle, cnt, m, n, ptr(fwd.a), ptr(fwd.s), ptr(fwd.perm),
+                                      ptr(fwd.rotors), fwd.rotor_cap, ptr(fwd.counts), ptr(ubar),
+                                      ptr(sbar), ptr(vbar), ptr(qbar), ptr(stored_vt), float(gap_tol),
+                                      ptr(ab), L.DEVICE_POINTERS)
+    else:
+        ab = np.empty((cnt, m, n))
+        p = lambda x: _ptr(_f64(x)) if x is not None else None  # noqa: E731
+        keep = [None if x is None else _f64(x) for x in (ubar, sbar, vbar, qbar, stored_vt)]
+        st = ctx.lib.lsvd_svd_vjp_f64(ctx.handle, cnt, m, n, _ptr(fwd.a), _ptr(fwd.s), _ptr(fwd.perm),
+                                      _ptr(fwd.rotors), fwd.rotor_cap, _ptr(fwd.counts),
+                                      *[_ptr(x) if x is not None else None for x in keep],
+                                      float(gap_tol), _ptr(ab), 0)
+        del p
+    _check(ctx.lib, ctx.handle, st, "svd_vjp")
+    return ab
