@@ -47,6 +47,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "SVDs/sec & polar TFLOP/s, mixed+refined vs plain FP64, at 1e-12 sigma rel err"
+# dram__bytes_read.sum + dram__bytes_write.sum of one batched_kernel launch on
+# 20,000 matrices of this workload (ncu --set full): 655.3 MB, i.e. per matrix
+NCU_DRAM_BYTES_PER_MATRIX = 655.3e6 / 20000
 WORKLOAD = "batched_uneven_svd_100k_n2-64_kappa1e0-1e12"
 
 
@@ -62,6 +65,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="batched workload on N GPUs: weak = a full batch per rank; strong = one "
+                         "batch split into cost-balanced contiguous shards")
     ap.add_argument("--workload", default="batched",
                     choices=["batched", "polar", "jade", "single", "adjoint"])
     ap.add_argument("--families", type=int, default=512)
@@ -267,8 +273,18 @@ def run_b200(args):
     from lie_cliffalg_analog_svd_b200 import _lib as L
     from lie_cliffalg_analog_svd_b200 import profiles as P
 
-    # weak scaling: every rank owns its own 100k-matrix shard
-    ns, a, sig = P.uneven_batch_workload(args.count, seed=args.seed + rank)
+    from lie_cliffalg_analog_svd_b200 import dist as D
+    if args.scaling == "weak":
+        # every rank owns its own full batch
+        ns, a, sig = P.uneven_batch_workload(args.count, seed=args.seed + rank)
+    else:
+        # one batch, cost-balanced contiguous shards (cost n^3)
+        ns_all, a_all, sig_all = P.uneven_batch_workload(args.count, seed=args.seed)
+        lo, hi = D.shard_bounds(ns_all.astype(np.float64) ** 3, ws, rank)
+        ao_all = np.concatenate([[0], np.cumsum(ns_all.astype(np.int64) ** 2)])
+        so_all = np.concatenate([[0], np.cumsum(ns_all.astype(np.int64))])
+        ns, a, sig = ns_all[lo:hi], a_all[ao_all[lo]:ao_all[hi]], sig_all[so_all[lo]:so_all[hi]]
+    local_count = int(ns.size)
     ctx = Context(local)
     stream = torch.cuda.Stream(device)
     ctx.set_stream(stream.cuda_stream)
@@ -278,7 +294,7 @@ def run_b200(args):
     out = (torch.empty(asz, dtype=torch.float64, device=device),
            torch.empty(ssz, dtype=torch.float64, device=device),
            torch.empty(asz, dtype=torch.float64, device=device),
-           torch.empty(args.count * 48, dtype=torch.uint8, device=device))
+           torch.empty(local_count * 48, dtype=torch.uint8, device=device))
     fp64_peak = fp64_peak_tflops(torch, device)
 
     # validation pass (untimed): accuracy against the imposed spectra
@@ -327,11 +343,9 @@ def run_b200(args):
         torch.distributed.barrier()
     ms = e0.elapsed_time(e1) / args.steps
     launches = ctx.kernel_launches - launches0
-    if ws > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = ws * args.count / (ms * 1e-3)
+    ms = D.max_over_ranks(ms, device)
+    units = ws * args.count if args.scaling == "weak" else args.count
+    value = units / (ms * 1e-3)
 
     # e2e through the C ABI with host (pinned) buffers
     e2e = None
@@ -347,12 +361,8 @@ def run_b200(args):
         t0 = time.perf_counter()
         for _ in range(args.steps):
             svd_batched(ns, a_h, precision=args.precision, ctx=ctx, out=outs_h)
-        el = (time.perf_counter() - t0) / args.steps
-        if ws > 1:
-            t = torch.tensor([el], dtype=torch.float64, device=device)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": ws * args.count / el, "unit": "SVDs/s",
+        el = D.max_over_ranks((time.perf_counter() - t0) / args.steps, device)
+        e2e = {"value": units / el, "unit": "SVDs/s",
                "h2d_bytes_per_step": int(a_h.nbytes),
                "d2h_bytes_per_step": int(outs_h[0].nbytes + outs_h[1].nbytes + outs_h[2].nbytes),
                "ms_per_step": el * 1e3}
@@ -360,7 +370,10 @@ def run_b200(args):
     peaks, peak_src = measured_peaks()
     achieved = flops / (ms * 1e-3) / 1e12
     roof = {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": fp64_peak,
-            "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+            "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+            "traffic": NCU_DRAM_BYTES_PER_MATRIX * local_count,
+            "traffic_source": "ncu dram bytes of batched_kernel on 20,000 matrices of this workload, "
+                              "scaled by the matrix count (per-matrix traffic: A in, U/S/Vt out)",
             "kernel": "lsvd::batched_kernel",
             "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul f64) measured in this run; "
                            "MEASURED_PEAKS.json holds no FP64 figure",
@@ -368,15 +381,17 @@ def run_b200(args):
             "hbm_gbs_peak": peaks.get("hbm_gbs"), "hbm_peak_source": peak_src}
     line = {"metric": METRIC, "value": value, "unit": "SVDs/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": args.scaling, "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else f"{args.precision}+f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "count_per_gpu": args.count, "n_range": [2, 64],
+            "config": {"workload": WORKLOAD,
+                       "count_per_gpu" if args.scaling == "weak" else "count_total": args.count,
+                       "n_range": [2, 64],
                        "kappa": "10^U[0,12]", "degenerate_fraction": 0.05,
                        "precision": args.precision,
                        "route": "LieSvdMicro (n<=4) / LieSvdSmall",
                        "l2": "inputs 1.1 GB per step, larger than the 126 MB L2",
-                       "parallelism": f"dp{ws} (independent shards)"},
+                       "parallelism": f"dp{ws} ({args.scaling} scaling, independent shards)"},
             "accuracy": acc, "roofline": roof, "gpu_launches": launches,
             "clocks": clk.summary(), "e2e": e2e,
             "polar_tflops": None}
@@ -412,11 +427,8 @@ def _init_dist():
 
 
 def _max_over_ranks(torch, ws, device, x):
-    if ws == 1:
-        return x
-    t = torch.tensor([x], dtype=torch.float64, device=device)
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return float(t.item())
+    from lie_cliffalg_analog_svd_b200 import dist as D
+    return D.max_over_ranks(x, device)
 
 
 POLAR_SHAPES = [(4096, 4096), (8192, 2048)]
