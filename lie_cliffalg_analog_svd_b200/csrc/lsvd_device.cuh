@@ -568,6 +568,13 @@ __device__ inline int jacobi2pp_sweeps(const Team& t, int n, double* B0, double*
     double* nxt = B1;
     int cp = 0;  // parity of sc->pidx describing cur
     const int lane = t.lane;
+    // The per-item indices below advance by t.nthreads each pass; their
+    // starts and steps are divided out once here, so the layer loops carry
+    // no integer division (runtime divisors cost ~20 instructions each).
+    const int p_a0 = (t.warp * 32 + lane) % half, p_b0 = (t.warp * 32 + lane) / half;
+    const int p_da = t.nthreads % half, p_db = t.nthreads / half;
+    const int v_i0 = n > 0 ? (t.warp * 32 + lane) % n : 0, v_b0 = n > 0 ? (t.warp * 32 + lane) / n : 0;
+    const int v_di = n > 0 ? t.nthreads % n : 0, v_db = n > 0 ? t.nthreads / n : 0;
     for (int sw = 0; sw < max_sweeps; ++sw) {
         sweeps = sw + 1;
         double off = 0.0;
@@ -622,9 +629,13 @@ __device__ inline int jacobi2pp_sweeps(const Team& t, int n, double* B0, double*
             }
             // P <- J^T P J into the next layer's positions
             const int nb = half * half;
-            for (int base = t.warp * 32; base < nb; base += t.nthreads) {
+            int a = p_a0, b = p_b0;
+            for (int base = t.warp * 32; base < nb; base += t.nthreads, a += p_da, b += p_db) {
+                if (a >= half) {
+                    a -= half;
+                    b++;
+                }
                 const int bi = base + lane;
-                const int a = bi % half, b = bi / half;
                 const double ca = __shfl_sync(0xffffffffu, c, a), sa = __shfl_sync(0xffffffffu, s, a);
                 const double cb = __shfl_sync(0xffffffffu, c, b & 31), sb = __shfl_sync(0xffffffffu, s, b & 31);
                 const double ta = __shfl_sync(0xffffffffu, tt, a);
@@ -658,9 +669,14 @@ __device__ inline int jacobi2pp_sweeps(const Team& t, int n, double* B0, double*
             }
             // V <- V J (natural order); item = (pair b, row i)
             const int nv = half * n;
-            for (int base = t.warp * 32; base < nv; base += t.nthreads) {
+            int vb = v_b0, vi_ = v_i0;
+            for (int base = t.warp * 32; base < nv; base += t.nthreads, vi_ += v_di, vb += v_db) {
+                if (vi_ >= n) {
+                    vi_ -= n;
+                    vb++;
+                }
                 const int vi = base + lane;
-                const int b = vi / n, i = vi - (vi / n) * n;
+                const int b = vb, i = vi_;
                 const double cb = __shfl_sync(0xffffffffu, c, b & 31), sb = __shfl_sync(0xffffffffu, s, b & 31);
                 if (vi >= nv) continue;
                 const int ib = sc->pidx[cp][2 * b], jb = sc->pidx[cp][2 * b + 1];
@@ -680,6 +696,264 @@ __device__ inline int jacobi2pp_sweeps(const Team& t, int n, double* B0, double*
     *Pout = cur;
     *par = cp;
     return sweeps;
+}
+
+// Blocked two-sided Jacobi for the same eigensolve (eigh_jacobi_full,
+// src/lie_svd_small.rs:212-285), used when no rotor stream is requested.
+// Indices are cut into blocks of B (8 for n >= 40, else 4) and the blocks
+// are paired by the circle method; in block layer l every block pair k owns
+// 2B indices.  One warp solves the 2B x 2B principal sub-block S_k of its
+// block pair: B rounds of B disjoint rotations (cross pairs; at layer 0 also
+// the B-1 rounds of pairs inside the blocks), each with the reference's
+// tangent, skip rule and exact diagonal update, accumulated into R_k.  The
+// team then applies all R_k at once, W = P R and V <- V R (rows of P and V,
+// in place, one (row, block pair) segment per item), then P' = R^T W
+// (columns, in place), writing the solved S_k on the diagonal tiles.  Every
+// index pair is visited once per sweep, as in the reference; the pair order
+// differs.  The P data in shared memory move once per block layer instead of
+// once per rotation layer, and R is applied with 2B FMAs per load.
+// P: natural order, column-major, leading dimension pld; scr: scratch of
+// nbp * 2 * (2B)^2 doubles.  Returns the sweeps started.
+__device__ inline int block_jacobi_fits(int n, int scr_doubles) {
+    const int B = n >= 40 ? 8 : 4, B2 = 2 * B;
+    const int nbl = (n + B - 1) / B, nbe = nbl + (nbl & 1);
+    // sub-blocks S, R per block pair, then the block-pair table (64 ints) and the
+    // per-warp rotation tables (8 ints + 16 double2 per warp, 8 warps)
+    return (nbe / 2) * 2 * B2 * (B2 + 2) + 64 + 256 <= scr_doubles && nbe >= 2 && (nbe / 2) * B <= 32;
+}
+
+// M[:, pair k columns] <- M[:, pair k columns] R_k for every block pair k of
+// the layer: one (row i, block pair k) segment per item, in place (the item
+// owns those 2B entries of row i).
+template <int B>
+__device__ __forceinline__ void seg_right_multiply(const Team& t, int n, int nbp, double* M, int ldm,
+                                                   const double* scr, const int* bp_lo, const int* bp_hi) {
+    constexpr int B2 = 2 * B, SLD = B2 + 2, BB = B2 * SLD;  // sub-block stride B2 + 2: conflict-free columns
+    const int nit = n * nbp;
+    int k = 0, i = t.tid;
+    while (i >= n) {
+        i -= n;
+        k++;
+    }
+    const int dk = t.nthreads / n, di = t.nthreads % n;
+    for (int it = t.tid; it < nit; it += t.nthreads, i += di, k += dk) {
+        if (i >= n) {
+            i -= n;
+            k++;
+        }
+        const int lo = bp_lo[k] * B, hi = bp_hi[k] * B - B;
+        const double* R = scr + k * 2 * BB + BB;
+        double x[B2];
+#pragma unroll
+        for (int cc = 0; cc < B2; ++cc) {
+            const int g = (cc < B ? lo : hi) + cc;
+            x[cc] = g < n ? M[g * ldm + i] : 0.0;
+        }
+#pragma unroll 1
+        for (int cc = 0; cc < B2; cc += 2) {
+            double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+            for (int cp = 0; cp < B2; ++cp) {
+                const double2 rr = *reinterpret_cast<const double2*>(R + cp * SLD + cc);
+                y0 = fma(x[cp], rr.x, y0);
+                y1 = fma(x[cp], rr.y, y1);
+            }
+            const int g0 = (cc < B ? lo : hi) + cc, g1 = g0 + 1;
+            if (g0 < n) M[g0 * ldm + i] = y0;
+            if (g1 < n) M[g1 * ldm + i] = y1;
+        }
+    }
+}
+
+template <int B>
+__device__ inline int jacobi_block_sweeps_t(const Team& t, int n, double* P, int pld, double* scr,
+                                            double* V, int ldv, double ref_norm, int max_sweeps,
+                                            TeamScratch* sc, long long* rotations, bool* capped) {
+    constexpr int B2 = 2 * B, SLD = B2 + 2, BB = B2 * SLD;  // sub-block stride B2 + 2: conflict-free columns
+    const int nbl = (n + B - 1) / B, nbe = nbl + (nbl & 1), nbp = nbe / 2, layers = nbe - 1;
+    const int lane = t.lane;
+    // block-pair table of the current layer: bp_lo[k], bp_hi[k] (block indices)
+    int* bp_lo = reinterpret_cast<int*>(scr + nbp * 2 * BB);
+    int* bp_hi = bp_lo + 32;
+    int sweeps = 0;
+    *capped = false;
+    for (int sw = 0; sw < max_sweeps; ++sw) {
+        sweeps = sw + 1;
+        double off = 0.0;
+        for (int y = t.warp; y < n; y += t.nwarps)
+            for (int x = lane; x < n; x += 32)
+                if (x != y) off = fma(P[y * pld + x], P[y * pld + x], off);
+        off = 0.5 * team_sum(t, off, sc->red);
+        if (sqrt(off) < 1e-13 * ref_norm) break;  // JACOBI_TOL, :69
+        if (sw + 1 == max_sweeps) *capped = true;
+        int nrot = 0;
+        for (int l = 0; l < layers; ++l) {
+            if (t.warp == 0 && lane < nbp) {
+                int A, Bk;
+                rr_pair(nbe, l, lane, A, Bk);
+                bp_lo[lane] = min(A, Bk);
+                bp_hi[lane] = max(A, Bk);
+            }
+            t.sync();
+            // ---- solve: one warp per block pair, warp-synchronous
+            for (int k = t.warp; k < nbp; k += t.nwarps) {
+                const int lo = bp_lo[k] * B, hi = bp_hi[k] * B;  // first global index of each block
+                double* S = scr + k * 2 * BB;
+                double* R = S + BB;
+#pragma unroll
+                for (int u = 0; u < B2 * B2 / 32; ++u) {
+                    const int e = lane + 32 * u;
+                    const int r = e / B2, c = e % B2;
+                    const int gr = (r < B ? lo : hi - B) + r, gc = (c < B ? lo : hi - B) + c;
+                    S[r * SLD + c] = (gr < n && gc < n) ? P[gc * pld + gr] : 0.0;
+                    R[r * SLD + c] = (r == c) ? 1.0 : 0.0;
+                }
+                __syncwarp();
+                const int rounds = B + (l == 0 ? B - 1 : 0);
+                for (int rd = 0; rd < rounds; ++rd) {
+                    const int lr = lane % B;
+                    int p, q;
+                    if (rd < B) {
+                        p = lr;
+                        q = B + (lr + rd) % B;
+                    } else {
+                        int x, y;
+                        rr_pair(B, rd - B, lr % (B / 2), x, y);
+                        const int o = lr < B / 2 ? 0 : B;
+                        p = o + min(x, y);
+                        q = o + max(x, y);
+                    }
+                    const int gp = (p < B ? lo : hi - B) + p, gq = (q < B ? lo : hi - B) + q;
+                    double c = 1.0, s = 0.0, npp = 0.0, nqq = 0.0;
+                    if (lane < B && gp < n && gq < n) {
+                        const double app = S[p * SLD + p], aqq = S[q * SLD + q], apq = S[p * SLD + q];
+                        npp = app;
+                        nqq = aqq;
+                        if (fabs(apq) >= 1e-300) {  // :232
+                            const double dd = aqq - app, g2 = 2.0 * apq;
+                            const double t0 = g2 / (fabs(dd) + sqrt(fma(dd, dd, g2 * g2)));
+                            const double tt = dd < 0.0 ? -t0 : t0;
+                            c = rsqrt(fma(tt, tt, 1.0));
+                            s = tt * c;
+                            npp = app - tt * apq;  // :244-249
+                            nqq = aqq + tt * apq;
+                            nrot++;
+                        }
+                    }
+                    // this round's rotations to a per-warp table (lanes < B), read
+                    // back by broadcast: rot_pq = p | q << 8, rot_cs = (c, s),
+                    // rot_nd = exact new diagonal (npp, nqq)
+                    int* rot_pq = bp_lo + 64 + t.warp * 8;
+                    double2* rot_cs = reinterpret_cast<double2*>(scr + nbp * 2 * BB + 64) + t.warp * 16;
+                    double2* rot_nd = rot_cs + 8;
+                    if (lane < B) {
+                        rot_pq[lane] = (s != 0.0) ? (p | (q << 8)) : -1;
+                        rot_cs[lane] = make_double2(c, s);
+                        rot_nd[lane] = make_double2(npp, nqq);
+                    }
+                    __syncwarp();
+                    // rows p, q of S: lane = (column, parity of the rotation index)
+                    {
+                        const int col = lane % B2;
+#pragma unroll
+                        for (int r = lane / B2; r < B; r += 32 / B2) {
+                            const int pq = rot_pq[r];
+                            if (pq < 0) continue;
+                            const int pr = pq & 255, qr = pq >> 8;
+                            const double2 cs = rot_cs[r];
+                            const double xv = S[pr * SLD + col], yv = S[qr * SLD + col];
+                            S[pr * SLD + col] = cs.x * xv - cs.y * yv;
+                            S[qr * SLD + col] = cs.y * xv + cs.x * yv;
+                        }
+                    }
+                    __syncwarp();
+                    // columns p, q of S and R: lane = (matrix, row)
+                    if (lane < 2 * B2) {
+                        const int mat = lane / B2, x = lane % B2;
+                        double* M = mat ? R : S;
+#pragma unroll
+                        for (int r = 0; r < B; ++r) {
+                            const int pq = rot_pq[r];
+                            if (pq < 0) continue;
+                            const int pr = pq & 255, qr = pq >> 8;
+                            const double2 cs = rot_cs[r];
+                            const double xv = M[x * SLD + pr], yv = M[x * SLD + qr];
+                            double vp = cs.x * xv - cs.y * yv, vq = cs.y * xv + cs.x * yv;
+                            if (!mat && (x == pr || x == qr)) {
+                                const double2 nd = rot_nd[r];
+                                vp = x == pr ? nd.x : 0.0;
+                                vq = x == pr ? 0.0 : nd.y;
+                            }
+                            M[x * SLD + pr] = vp;
+                            M[x * SLD + qr] = vq;
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            t.sync();
+            // ---- apply, pass 1: W = P R and V <- V R, one (row, block pair) segment per item
+            const int nit = n * nbp;
+            seg_right_multiply<B>(t, n, nbp, P, pld, scr, bp_lo, bp_hi);
+            seg_right_multiply<B>(t, n, nbp, V, ldv, scr, bp_lo, bp_hi);
+            t.sync();
+            // ---- apply, pass 2: P' = R^T W, one (column, block pair) segment per item
+            {
+                int k = 0, j = t.tid;
+                while (j >= n) {
+                    j -= n;
+                    k++;
+                }
+                const int dk = t.nthreads / n, dj = t.nthreads % n;
+                for (int it = t.tid; it < nit; it += t.nthreads, j += dj, k += dk) {
+                    if (j >= n) {
+                        j -= n;
+                        k++;
+                    }
+                    const int blo = bp_lo[k], bhi = bp_hi[k];
+                    const int lo = blo * B, hi = bhi * B - B;
+                    const double* S = scr + k * 2 * BB;
+                    const double* R = S + BB;
+                    const int jb = j / B;
+                    const int jloc = jb == blo ? j - lo : (jb == bhi ? j - hi : -1);
+                    double x[B2];
+#pragma unroll
+                    for (int r = 0; r < B2; ++r) {
+                        const int g = (r < B ? lo : hi) + r;
+                        x[r] = g < n ? P[j * pld + g] : 0.0;
+                    }
+#pragma unroll 1
+                    for (int r = 0; r < B2; r += 2) {
+                        double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+                        for (int rp = 0; rp < B2; ++rp) {
+                            const double2 rr = *reinterpret_cast<const double2*>(R + rp * SLD + r);
+                            y0 = fma(rr.x, x[rp], y0);
+                            y1 = fma(rr.y, x[rp], y1);
+                        }
+                        if (jloc >= 0) {  // diagonal tile: the solved sub-block
+                            y0 = S[r * SLD + jloc];
+                            y1 = S[(r + 1) * SLD + jloc];
+                        }
+                        const int g0 = (r < B ? lo : hi) + r, g1 = g0 + 1;
+                        if (g0 < n) P[j * pld + g0] = y0;
+                        if (g1 < n) P[j * pld + g1] = y1;
+                    }
+                }
+            }
+            t.sync();
+        }
+        *rotations += (long long)team_sum(t, double(nrot), sc->red);
+    }
+    return sweeps;
+}
+
+__device__ inline int jacobi_block_sweeps(const Team& t, int n, double* P, int pld, double* scr,
+                                          double* V, int ldv, double ref_norm, int max_sweeps,
+                                          TeamScratch* sc, long long* rotations, bool* capped) {
+    if (n >= 40)
+        return jacobi_block_sweeps_t<8>(t, n, P, pld, scr, V, ldv, ref_norm, max_sweeps, sc, rotations, capped);
+    return jacobi_block_sweeps_t<4>(t, n, P, pld, scr, V, ldv, ref_norm, max_sweeps, sc, rotations, capped);
 }
 
 // LieSvdSmall::solve (src/lie_svd_small.rs:296-323) by one team, n <= 64.
@@ -817,12 +1091,18 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     // of the ping-pong buffer Vb (leading dimension m); Q is parked in the U
     // output (global) so that Q's buffer can be the second ping-pong buffer.
     const int m = (n % 2 == 0) ? n : n + 1;
+    // Without a rotor stream to record, n >= 48 takes the blocked sweep (P in
+    // natural order, odd leading dimension m + 1); otherwise the layer-by-
+    // layer sweep with P in pair-position order (leading dimension m).  The
+    // threshold is where the blocked sweep overtakes (measured on B200).
+    const bool blocked = job.rotors == nullptr && n >= 48 && block_jacobi_fits(n, ld * np);
+    const int pstride = blocked ? m + 1 : m;
     for (int x = t.tid; x < m; x += t.nthreads) {
         // layer 0: pair k = (m-1, 0) for k = 0, else (k, m-1-k) in ring m-1
         const int k = x >> 1;
         int a = k == 0 ? m - 1 : k, bb = k == 0 ? 0 : (m - 1 - k) % (m - 1);
         const int lo = min(a, bb), hi = max(a, bb);
-        sc->pidx[0][x] = (x & 1) ? hi : lo;
+        sc->pidx[0][x] = blocked ? x : ((x & 1) ? hi : lo);
     }
     for (int idx = t.tid; idx < n * n; idx += t.nthreads) {
         const int i = idx / n, j = idx % n;
@@ -835,7 +1115,7 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
         const int i = sc->pidx[0][x], j = sc->pidx[0][y];
         double v = 0.0;
         if (i < n && j < n) v = (Wb[j * ld + i] + Wb[i * ld + j]) * 0.5;
-        Vb[y * m + x] = v;
+        Vb[y * pstride + x] = v;
         pf2 = fma(v, v, pf2);
     }
     const double pref = fmax(sqrt(team_sum(t, pf2, sc->red)), 1e-300);  // syncs Vb
@@ -853,8 +1133,16 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     bool jcap = false;
     double* Pfin = nullptr;
     int par = 0;
-    const int sweeps = jacobi2pp_sweeps(t, n, Vb, Q, Vn, ld, pref, 60 + 20 * n /* :216 */, sc, job,
-                                        &rotations, &jcap, &Pfin, &par);
+    int sweeps;
+    if (blocked) {
+        sweeps = jacobi_block_sweeps(t, n, Vb, pstride, Q, Vn, ld, pref, 60 + 20 * n /* :216 */, sc,
+                                     &rotations, &jcap);
+        Pfin = Vb;
+        par = 0;
+    } else {
+        sweeps = jacobi2pp_sweeps(t, n, Vb, Q, Vn, ld, pref, 60 + 20 * n /* :216 */, sc, job, &rotations,
+                                  &jcap, &Pfin, &par);
+    }
     if (jcap) flags |= LSVD_MAT_JACOBI_CAP;
     double* const Pother = (Pfin == Vb) ? Q : Vb;
     Vb = Vn;
@@ -862,7 +1150,7 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     // ---- eigenvalues on the diagonal, stable descending sort, sigma = max(eig, 0)
     for (int x = t.tid; x < m; x += t.nthreads) {
         const int i = sc->pidx[par][x];
-        if (i < n) sc->sig[i] = Pfin[x * m + x];
+        if (i < n) sc->sig[i] = Pfin[x * pstride + x];
     }
     t.sync();
     for (int j = t.tid; j < n; j += t.nthreads) {
