@@ -44,6 +44,10 @@ namespace {
 
 constexpr int B = 8;        // block size
 constexpr int B2 = 2 * B;   // indices of a block pair
+// Shared sub-block layout of the solve kernel: row stride B2 + 1 and matrix
+// stride B2 (B2 + 1) + 1 doubles, so that lanes walking a column, or the same
+// entry of consecutive matrices, fall in different banks.
+constexpr int SLD = B2 + 1, MST = B2 * SLD + 1;
 constexpr int kThreads = 256;
 constexpr double kPi = 3.141592653589793238462643383279502884;
 
@@ -118,14 +122,15 @@ __global__ void __launch_bounds__(kThreads, 1) jade_solve_kernel(JadeArgs a) {
     __syncthreads();
     const int K = a.K, n = a.n;
     double* S = sh;                    // S[k][r][c]
-    double* Rs = sh + size_t(K) * B2 * B2;
+    double* Rs = sh + size_t(K) * MST;
     const double* Wf = a.W + size_t(f) * K * n * n;
     for (int e = tid; e < K * B2 * B2; e += kThreads) {
         const int k = e / (B2 * B2), r = (e / B2) % B2, c = e % B2;
+        const int se = k * MST + r * SLD + c;
         const int gi = idx[r], gj = idx[c];
-        S[e] = (gi >= 0 && gj >= 0) ? Wf[(size_t(k) * n + gi) * n + gj] : 0.0;
+        S[se] = (gi >= 0 && gj >= 0) ? Wf[(size_t(k) * n + gi) * n + gj] : 0.0;
     }
-    for (int e = tid; e < B2 * B2; e += kThreads) Rs[e] = (e / B2 == e % B2) ? 1.0 : 0.0;
+    for (int e = tid; e < B2 * B2; e += kThreads) Rs[(e / B2) * SLD + e % B2] = (e / B2 == e % B2) ? 1.0 : 0.0;
     __syncthreads();
     const double ptol = a.pair_tol[f];
     const int rounds_cross = B, rounds_intra = (a.layer == 0) ? B - 1 : 0;
@@ -156,10 +161,10 @@ __global__ void __launch_bounds__(kThreads, 1) jade_solve_kernel(JadeArgs a) {
             double poff = 0.0, sxx = 0.0, syy = 0.0, sxy = 0.0;
             if (valid)
                 for (int k = lane; k < K; k += 32) {
-                    const double* Sk = S + size_t(k) * B2 * B2;
-                    const double mij = Sk[li * B2 + lj], mji = Sk[lj * B2 + li];
+                    const double* Sk = S + size_t(k) * MST;
+                    const double mij = Sk[li * SLD + lj], mji = Sk[lj * SLD + li];
                     poff += fabs(mij) + fabs(mji);
-                    const double x = 0.5 * (Sk[li * B2 + li] - Sk[lj * B2 + lj]);
+                    const double x = 0.5 * (Sk[li * SLD + li] - Sk[lj * SLD + lj]);
                     const double y = 0.5 * (mij + mji);
                     sxx += x * x;
                     syy += y * y;
@@ -179,19 +184,19 @@ __global__ void __launch_bounds__(kThreads, 1) jade_solve_kernel(JadeArgs a) {
                 sincos(alt, &sa, &ca);
                 double et = 0.0, ea = 0.0, before = 0.0;
                 for (int k = lane; k < K; k += 32) {
-                    const double* Sk = S + size_t(k) * B2 * B2;
-                    const double av = Sk[li * B2 + li], dv = Sk[lj * B2 + lj];
-                    const double bv = 0.5 * (Sk[li * B2 + lj] + Sk[lj * B2 + li]);
+                    const double* Sk = S + size_t(k) * MST;
+                    const double av = Sk[li * SLD + li], dv = Sk[lj * SLD + lj];
+                    const double bv = 0.5 * (Sk[li * SLD + lj] + Sk[lj * SLD + li]);
                     const double ot = 0.5 * (av - dv) * (2.0 * st * ct) + bv * (ct * ct - st * st);
                     const double oa = 0.5 * (av - dv) * (2.0 * sa * ca) + bv * (ca * ca - sa * sa);
                     et += 2.0 * ot * ot;
                     ea += 2.0 * oa * oa;
                     // local_offdiag_sq_for_axes (:475-494) restricted to the sub-block
                     for (int c = 0; c < B2; ++c) {
-                        if (c != li) before += Sk[li * B2 + c] * Sk[li * B2 + c];
-                        if (c != lj) before += Sk[lj * B2 + c] * Sk[lj * B2 + c];
+                        if (c != li) before += Sk[li * SLD + c] * Sk[li * SLD + c];
+                        if (c != lj) before += Sk[lj * SLD + c] * Sk[lj * SLD + c];
                         if (c != li && c != lj)
-                            before += Sk[c * B2 + li] * Sk[c * B2 + li] + Sk[c * B2 + lj] * Sk[c * B2 + lj];
+                            before += Sk[c * SLD + li] * Sk[c * SLD + li] + Sk[c * SLD + lj] * Sk[c * SLD + lj];
                     }
                 }
                 et = warp_sum(et);
@@ -209,9 +214,9 @@ __global__ void __launch_bounds__(kThreads, 1) jade_solve_kernel(JadeArgs a) {
                         sincos(theta * scale, &s, &c);
                         double delta = 0.0;
                         for (int k = lane; k < K; k += 32) {
-                            const double* Sk = S + size_t(k) * B2 * B2;
-                            const double m00 = Sk[li * B2 + li], m01 = Sk[li * B2 + lj];
-                            const double m10 = Sk[lj * B2 + li], m11 = Sk[lj * B2 + lj];
+                            const double* Sk = S + size_t(k) * MST;
+                            const double m00 = Sk[li * SLD + li], m01 = Sk[li * SLD + lj];
+                            const double m10 = Sk[lj * SLD + li], m11 = Sk[lj * SLD + lj];
                             // rows then columns (apply_symmetric_rotor, :401-404)
                             const double r00 = c * m00 - s * m10, r01 = c * m01 - s * m11;
                             const double r10 = s * m00 + c * m10, r11 = s * m01 + c * m11;
@@ -248,11 +253,11 @@ __global__ void __launch_bounds__(kThreads, 1) jade_solve_kernel(JadeArgs a) {
             const double s = ps[p];
             if (s == 0.0) continue;
             const double c = pc[p];
-            double* Sk = S + size_t(k) * B2 * B2;
+            double* Sk = S + size_t(k) * MST;
             const int li = pl[p], lj = pm[p];
-            const double x = Sk[li * B2 + col], y = Sk[lj * B2 + col];
-            Sk[li * B2 + col] = c * x - s * y;
-            Sk[lj * B2 + col] = s * x + c * y;
+            const double x = Sk[li * SLD + col], y = Sk[lj * SLD + col];
+            Sk[li * SLD + col] = c * x - s * y;
+            Sk[lj * SLD + col] = s * x + c * y;
         }
         __syncthreads();
         // columns (apply_right_rotor, :417-426) and the basis (apply_basis_rotor, :428-437)
@@ -261,15 +266,15 @@ __global__ void __launch_bounds__(kThreads, 1) jade_solve_kernel(JadeArgs a) {
             const double s = ps[p];
             if (s == 0.0) continue;
             const double c = pc[p];
-            double* Sk = k < K ? S + size_t(k) * B2 * B2 : Rs;
+            double* Sk = k < K ? S + size_t(k) * MST : Rs;
             const int li = pl[p], lj = pm[p];
-            const double x = Sk[row * B2 + li], y = Sk[row * B2 + lj];
-            Sk[row * B2 + li] = c * x - s * y;
-            Sk[row * B2 + lj] = s * x + c * y;
+            const double x = Sk[row * SLD + li], y = Sk[row * SLD + lj];
+            Sk[row * SLD + li] = c * x - s * y;
+            Sk[row * SLD + lj] = s * x + c * y;
         }
         __syncthreads();
     }
-    for (int e = tid; e < B2 * B2; e += kThreads) R[e] = Rs[e];
+    for (int e = tid; e < B2 * B2; e += kThreads) R[e] = Rs[(e / B2) * SLD + e % B2];
     if (tid == 0) {
         atomicAdd((unsigned long long*)&a.rot[2 * f], (unsigned long long)nacc);
         atomicAdd((unsigned long long*)&a.rot[2 * f + 1], (unsigned long long)nrej);
@@ -399,9 +404,9 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
     if (families == 0) return LSVD_OK;
     if (K == 0) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "LieSvdJoint: empty matrix set");
     if (!M || !V || !diag || !traces) return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "null pointer");
-    const size_t smem = size_t(K) * B2 * B2 * 8 + B2 * B2 * 8;
+    const size_t smem = size_t(K) * MST * 8 + B2 * SLD * 8;
     if (smem > 200 * 1024 || n > 32768)
-        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "LieSvdJoint: K must be <= 99 (shared memory)");
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "LieSvdJoint: K must be <= 93 (shared memory)");
     const lsvd_joint_params p = params ? *params : lsvd_joint_params_for_n(n);
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
