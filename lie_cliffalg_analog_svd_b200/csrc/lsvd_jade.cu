@@ -281,53 +281,122 @@ __global__ void __launch_bounds__(kThreads, 1) jade_solve_kernel(JadeArgs a) {
     }
 }
 
-// grid (nbp, K + 1, F): row block pair P of matrix k (k == K: the basis V).
-// Every tile M[P, Q] <- R_P^T M[P, Q] R_Q (for V: V[:, Q] <- V[:, Q] R_Q).
+// grid (K + 1, F), kThreads: matrix k of family f (k == K: the basis V).
+// M <- R^T M R with R = blockdiag over the layer's block pairs (for V:
+// V <- V R), streamed one strip of 2B rows (a row block pair P) at a time:
+//   load  : each thread takes columns, reads the strip's 2B rows from global
+//           (coalesced) into registers and left-multiplies by R_P^T;
+//   stage : the product goes to a shared strip (row stride n + 1);
+//   right : one warp per column block pair Q; lane (rr, quarter) holds rows
+//           rr and rr + B and 4 of the 2B columns, R_Q read as 16-byte
+//           broadcasts; results in place (each lane owns its entries);
+//   store : coalesced row stores back to global.
+// All R of the family sit in shared memory for the whole matrix, so M's data
+// cross HBM once per layer.  Positions past n are padding (R is the
+// identity there and they are never loaded or stored).
+__device__ __forceinline__ int jade_pos(int blk_lo, int blk_hi, int pos, int n) {
+    const int g = (pos < B ? blk_lo : blk_hi) * B + (pos % B);
+    return g < n ? g : -1;
+}
+
 __global__ void __launch_bounds__(kThreads) jade_apply_kernel(JadeArgs a) {
-    const int P = blockIdx.x, k = blockIdx.y, f = blockIdx.z;
+    const int k = blockIdx.x, f = blockIdx.y;
     if (!a.active[f]) return;
-    const int nbp = a.nbe / 2, n = a.n;
-    __shared__ double RP[B2 * B2], RQ[B2 * B2], T[B2 * B2], X[B2 * B2];
-    __shared__ int ip[B2], iq[B2];
-    const int tid = threadIdx.x, r = tid / B2, c = tid % B2;
+    extern __shared__ __align__(16) double ash[];
+    const int n = a.n, nbp = a.nbe / 2, ldt = n + 1;
     const bool isV = k == a.K;
     double* M = isV ? a.V + size_t(f) * n * n : a.W + (size_t(f) * a.K + k) * n * n;
-    if (tid < B2) {
+    double* Rall = ash;                              // nbp * B2 * B2
+    double* T = Rall + size_t(nbp) * B2 * B2;        // B2 x ldt
+    int* blo = reinterpret_cast<int*>(T + size_t(B2) * ldt);
+    int* bhi = blo + 32 * 4;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double* Rg = a.R + size_t(f) * nbp * B2 * B2;
+    for (int e = tid; e < nbp * B2 * B2; e += kThreads) Rall[e] = Rg[e];
+    for (int q = tid; q < nbp; q += kThreads) {
         int A, Bb;
-        rr_pair(a.nbe, a.layer, P, A, Bb);
-        const int lo = min(A, Bb), hi = max(A, Bb);
-        const int t = tid % B;
-        const int g = (tid < B ? lo : hi) * B + t;
-        ip[tid] = g < n ? g : -1;
+        rr_pair(a.nbe, a.layer, q, A, Bb);
+        blo[q] = min(A, Bb);
+        bhi[q] = max(A, Bb);
     }
-    RP[tid] = a.R[(size_t(f) * nbp + P) * B2 * B2 + tid];
     __syncthreads();
-    for (int Q = 0; Q < nbp; ++Q) {
-        if (tid < B2) {
-            int A, Bb;
-            rr_pair(a.nbe, a.layer, Q, A, Bb);
-            const int lo = min(A, Bb), hi = max(A, Bb);
-            const int t = tid % B;
-            const int g = (tid < B ? lo : hi) * B + t;
-            iq[tid] = g < n ? g : -1;
+    for (int P = 0; P < nbp; ++P) {
+        const int plo = blo[P], phi = bhi[P];
+        const double* RP = Rall + size_t(P) * B2 * B2;
+        // ---- load + left multiply (V: plain copy)
+        for (int col = tid; col < n; col += kThreads) {
+            double x[B2];
+#pragma unroll
+            for (int r = 0; r < B2; ++r) {
+                const int g = jade_pos(plo, phi, r, n);
+                x[r] = g >= 0 ? M[size_t(g) * n + col] : 0.0;
+            }
+            if (isV) {
+#pragma unroll
+                for (int r = 0; r < B2; ++r) T[r * ldt + col] = x[r];
+            } else {
+#pragma unroll 1
+                for (int r = 0; r < B2; r += 2) {
+                    double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+                    for (int rp = 0; rp < B2; ++rp) {
+                        const double2 rr = *reinterpret_cast<const double2*>(RP + rp * B2 + r);
+                        y0 = fma(rr.x, x[rp], y0);
+                        y1 = fma(rr.y, x[rp], y1);
+                    }
+                    T[r * ldt + col] = y0;
+                    T[(r + 1) * ldt + col] = y1;
+                }
+            }
         }
-        RQ[tid] = a.R[(size_t(f) * nbp + Q) * B2 * B2 + tid];
         __syncthreads();
-        const int gi = ip[r], gj = iq[c];
-        X[tid] = (gi >= 0 && gj >= 0) ? M[size_t(gi) * n + gj] : 0.0;
-        __syncthreads();
-        double t = 0.0;
-        for (int x = 0; x < B2; ++x) t = fma(X[r * B2 + x], RQ[x * B2 + c], t);
-        T[tid] = t;
-        __syncthreads();
-        double o;
-        if (isV) {
-            o = t;
-        } else {
-            o = 0.0;
-            for (int y = 0; y < B2; ++y) o = fma(RP[y * B2 + r], T[y * B2 + c], o);
+        // ---- right multiply by R_Q, in place in the strip
+        {
+            const int rr = lane % B, c0 = 4 * (lane / B);  // rows rr, rr + B; columns c0 .. c0 + 3
+            for (int Q = warp; Q < nbp; Q += kThreads / 32) {
+                const int qlo = blo[Q], qhi = bhi[Q];
+                const double* RQ = Rall + size_t(Q) * B2 * B2;
+                double x0[B2], x1[B2];
+#pragma unroll
+                for (int c = 0; c < B2; ++c) {
+                    const int g = jade_pos(qlo, qhi, c, n);
+                    x0[c] = g >= 0 ? T[rr * ldt + g] : 0.0;
+                    x1[c] = g >= 0 ? T[(rr + B) * ldt + g] : 0.0;
+                }
+                double y0[4] = {0.0, 0.0, 0.0, 0.0}, y1[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                for (int cp = 0; cp < B2; ++cp) {
+                    const double2 ra = *reinterpret_cast<const double2*>(RQ + cp * B2 + c0);
+                    const double2 rb = *reinterpret_cast<const double2*>(RQ + cp * B2 + c0 + 2);
+                    y0[0] = fma(x0[cp], ra.x, y0[0]);
+                    y0[1] = fma(x0[cp], ra.y, y0[1]);
+                    y0[2] = fma(x0[cp], rb.x, y0[2]);
+                    y0[3] = fma(x0[cp], rb.y, y0[3]);
+                    y1[0] = fma(x1[cp], ra.x, y1[0]);
+                    y1[1] = fma(x1[cp], ra.y, y1[1]);
+                    y1[2] = fma(x1[cp], rb.x, y1[2]);
+                    y1[3] = fma(x1[cp], rb.y, y1[3]);
+                }
+                __syncwarp();  // every lane of the warp read its rows before any writes
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int g = jade_pos(qlo, qhi, c0 + u, n);
+                    if (g >= 0) {
+                        T[rr * ldt + g] = y0[u];
+                        T[(rr + B) * ldt + g] = y1[u];
+                    }
+                }
+            }
         }
-        if (gi >= 0 && gj >= 0) M[size_t(gi) * n + gj] = o;
+        __syncthreads();
+        // ---- store the strip
+        for (int col = tid; col < n; col += kThreads) {
+#pragma unroll
+            for (int r = 0; r < B2; ++r) {
+                const int g = jade_pos(plo, phi, r, n);
+                if (g >= 0) M[size_t(g) * n + col] = T[r * ldt + col];
+            }
+        }
         __syncthreads();
     }
 }
@@ -459,6 +528,13 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
     if ((e = cudaFuncSetAttribute(jade_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem))) != cudaSuccess)
         return lsvd_ctx_cuda(ctx, e, "jade smem");
+    // apply: all R of a family + one strip of 2B rows (row stride n + 1) + block tables
+    const size_t asmem = size_t(nbp) * B2 * B2 * 8 + size_t(B2) * (n + 1) * 8 + 2 * 32 * 4 * 4;
+    if (asmem > 200 * 1024)
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "LieSvdJoint: n too large for the apply pass");
+    if ((e = cudaFuncSetAttribute(jade_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(asmem))) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "jade apply smem");
     JadeArgs a;
     a.F = F;
     a.K = int(K);
@@ -480,7 +556,7 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
         for (int l = 0; l < layers; ++l) {
             a.layer = l;
             jade_solve_kernel<<<dim3(nbp, F), kThreads, smem, st>>>(a);
-            jade_apply_kernel<<<dim3(nbp, unsigned(K + 1), F), kThreads, 0, st>>>(a);
+            jade_apply_kernel<<<dim3(unsigned(K + 1), F), kThreads, asmem, st>>>(a);
             ctx->launches += 2;
         }
         jade_norms_kernel<<<F, kThreads, 0, st>>>(F, int(K), int(n), dW, active, off2, all2);
