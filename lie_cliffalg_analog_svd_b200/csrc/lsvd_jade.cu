@@ -83,6 +83,7 @@ struct JadeArgs {
     double* R;               // F*(nbe/2)*B2*B2
     long long* rot;          // per family: accepted, rejected
     const int* active;       // per family
+    double* part;            // last layer of a sweep: per matrix (offdiag^2, all^2), else null
 };
 
 // Block pair (A, Bk) of `layer` -> the 16 global indices (B of block A, then
@@ -299,7 +300,7 @@ __device__ __forceinline__ int jade_pos(int blk_lo, int blk_hi, int pos, int n) 
     return g < n ? g : -1;
 }
 
-__global__ void __launch_bounds__(kThreads) jade_apply_kernel(JadeArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) jade_apply_kernel(JadeArgs a) {
     const int k = blockIdx.x, f = blockIdx.y;
     if (!a.active[f]) return;
     extern __shared__ __align__(16) double ash[];
@@ -311,6 +312,7 @@ __global__ void __launch_bounds__(kThreads) jade_apply_kernel(JadeArgs a) {
     int* blo = reinterpret_cast<int*>(T + size_t(B2) * ldt);
     int* bhi = blo + 32 * 4;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double sum_off = 0.0, sum_all = 0.0;
     const double* Rg = a.R + size_t(f) * nbp * B2 * B2;
     for (int e = tid; e < nbp * B2 * B2; e += kThreads) Rall[e] = Rg[e];
     for (int q = tid; q < nbp; q += kThreads) {
@@ -389,16 +391,58 @@ __global__ void __launch_bounds__(kThreads) jade_apply_kernel(JadeArgs a) {
             }
         }
         __syncthreads();
-        // ---- store the strip
+        // ---- store the strip (last layer of a sweep: also the squared norms
+        // of the new matrix, joint_offdiag_norm / joint_frobenius_norm terms)
         for (int col = tid; col < n; col += kThreads) {
 #pragma unroll
             for (int r = 0; r < B2; ++r) {
                 const int g = jade_pos(plo, phi, r, n);
-                if (g >= 0) M[size_t(g) * n + col] = T[r * ldt + col];
+                if (g >= 0) {
+                    const double v = T[r * ldt + col];
+                    M[size_t(g) * n + col] = v;
+                    sum_all = fma(v, v, sum_all);
+                    if (g != col) sum_off = fma(v, v, sum_off);
+                }
             }
         }
         __syncthreads();
     }
+    if (a.part && !isV) {
+        // per-matrix partials in a fixed reduction order (deterministic)
+        __shared__ double red[2][kThreads / 32];
+        for (int o = 16; o > 0; o >>= 1) {
+            sum_off += __shfl_xor_sync(0xffffffffu, sum_off, o);
+            sum_all += __shfl_xor_sync(0xffffffffu, sum_all, o);
+        }
+        if (lane == 0) {
+            red[0][warp] = sum_off;
+            red[1][warp] = sum_all;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double so = 0.0, sa = 0.0;
+            for (int w = 0; w < kThreads / 32; ++w) {
+                so += red[0][w];
+                sa += red[1][w];
+            }
+            a.part[2 * (size_t(f) * a.K + k)] = so;
+            a.part[2 * (size_t(f) * a.K + k) + 1] = sa;
+        }
+    }
+}
+
+// off2[f], all2[f] = sums of the K per-matrix partials, in order.
+__global__ void jade_part_sum_kernel(int F, int K, const double* part, const int* active, double* off2,
+                                     double* all2) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F || !active[f]) return;
+    double so = 0.0, sa = 0.0;
+    for (int k = 0; k < K; ++k) {
+        so += part[2 * (size_t(f) * K + k)];
+        sa += part[2 * (size_t(f) * K + k) + 1];
+    }
+    off2[f] = so;
+    all2[f] = sa;
 }
 
 // Per family: sum over k, i != j of m_ij^2 (joint_offdiag_norm^2, :439-441)
@@ -488,7 +532,8 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
     // workspace: W (work copy) | V | R | off2, all2, tol | rot | active
     const size_t rsz = size_t(F) * nbp * B2 * B2;
     auto al = [](size_t x) { return (x + 31) & ~size_t(31); };
-    const size_t bytes = 8 * (al(wsz) + (dev ? 0 : al(vsz)) + al(rsz) + 4 * al(F)) + 16 * al(F) + 4 * al(F);
+    const size_t psz = 2 * size_t(F) * K;  // per-matrix norm partials of the last layer
+    const size_t bytes = 8 * (al(wsz) + (dev ? 0 : al(vsz)) + al(rsz) + 4 * al(F) + al(psz)) + 16 * al(F) + 4 * al(F);
     char* ws = static_cast<char*>(ctx->ws_rot.get(bytes, &e));
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "jade workspace");
     char* q = ws;
@@ -496,6 +541,7 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
     double* dV = dev ? V : reinterpret_cast<double*>(q);
     if (!dev) q += 8 * al(vsz);
     double* dR = reinterpret_cast<double*>(q); q += 8 * al(rsz);
+    double* dPart = reinterpret_cast<double*>(q); q += 8 * al(psz);
     double* off2 = reinterpret_cast<double*>(q); q += 8 * al(F);
     double* all2 = reinterpret_cast<double*>(q); q += 8 * al(F);
     double* ptol = reinterpret_cast<double*>(q); q += 8 * al(F);
@@ -547,6 +593,7 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
     a.R = dR;
     a.rot = rot;
     a.active = active;
+    a.part = nullptr;
     std::vector<double> before(h_init);
     int live = 0;
     for (int f = 0; f < F; ++f) live += h_act[f];
@@ -555,11 +602,13 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
             if (h_act[f]) h_sweeps[f] = sw + 1;
         for (int l = 0; l < layers; ++l) {
             a.layer = l;
+            a.part = (l + 1 == layers) ? dPart : nullptr;
             jade_solve_kernel<<<dim3(nbp, F), kThreads, smem, st>>>(a);
             jade_apply_kernel<<<dim3(unsigned(K + 1), F), kThreads, asmem, st>>>(a);
             ctx->launches += 2;
         }
-        jade_norms_kernel<<<F, kThreads, 0, st>>>(F, int(K), int(n), dW, active, off2, all2);
+        // the sweep's norms came out of the last layer's apply pass
+        jade_part_sum_kernel<<<(F + 127) / 128, 128, 0, st>>>(F, int(K), dPart, active, off2, all2);
         ctx->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "jade sweep");
         if ((e = cudaMemcpyAsync(h_off.data(), off2, 8 * F, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
