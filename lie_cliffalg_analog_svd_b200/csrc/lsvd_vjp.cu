@@ -14,7 +14,7 @@
 // Adjoint (lsvd_svd_vjp_f64): from A, sigma, perm and the stream alone, one
 // CTA per matrix
 //   * rebuilds V by replaying the stream in reverse, V = G_1 (G_2 (... (G_k P))),
-//     round by round (the rotations of one round are disjoint);
+//     one column per thread (rotations act on rows, so columns are independent);
 //   * applies the analytic thin-SVD adjoint, with U = A V S^-1 recomputed
 //     (not stored):
 //       Abar = U [F o (G - G^T) S + diag(Sbar) + S F o (H - H^T)] V^T
@@ -48,6 +48,7 @@ using lsvd::kMaxN;
 using lsvd::Team;
 
 constexpr int kVjpThreads = 256;
+constexpr int kChunk = 1024;  // rotations staged in shared memory per replay chunk
 constexpr int kMaxRows = 4096;
 
 __device__ double block_sum(double v, double* red) {
@@ -233,9 +234,10 @@ __global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
     double* S4 = S3 + n * ld;
     double* sg = S4 + n * ld;    // sigma
     double* si = sg + kMaxN;     // 1/sigma
-    __shared__ int grp_lo, grp_bad;
-    __shared__ double g_c[32], g_s[32];
-    __shared__ int g_i[32], g_j[32];
+    __shared__ int grp_bad;
+    __shared__ double2 g_cs[kChunk];
+    __shared__ int g_ij[kChunk];
+    __shared__ int g_safe[kChunk / 4];
     const int tid = threadIdx.x;
     const double* A = a.A + mi * size_t(m) * n;
     const double* Ub = a.Ub ? a.Ub + mi * size_t(m) * n : nullptr;
@@ -266,41 +268,65 @@ __global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
         if (tid == 0) a.status[mi] = grp_bad;
         return;
     }
-    // ---- V = G_1 (G_2 (... (G_k P))): rounds from the last one back, each
-    // a set of disjoint row rotations (rows i, j: c x_i + s x_j, -s x_i + c x_j)
+    // ---- V = G_1 (G_2 (... (G_k P))): the stream replayed from its end.  A
+    // rotation only mixes rows i and j of each column, so the thread that owns
+    // column `col` replays the whole stream on it with no barrier; the stream
+    // comes through shared memory in chunks with cos/sin computed once.
     const lsvd_rotor* rot = a.rotors + mi * size_t(a.cap);
-    int64_t hi = Vst ? 0 : cnt;  // the current group is [grp_lo, hi)
-    while (hi > 0) {
-        if (tid < 32) {
-            // a round holds at most n/2 <= 32 disjoint rotations: the group is
-            // the run of entries hi-1, hi-2, ... that share the last round
-            const uint32_t last = rot[hi - 1].round;
-            const int64_t e = hi - 1 - tid;
-            lsvd_rotor r;
-            r.round = ~last;
-            if (e >= 0) r = rot[e];
-            const unsigned ball = __ballot_sync(0xffffffffu, e >= 0 && r.round == last);
-            const int len = (~ball) ? __ffs(~ball) - 1 : 32;
-            if (tid < len) {
-                double sn, cs;
-                sincos(r.theta, &sn, &cs);
-                g_c[tid] = cs;
-                g_s[tid] = sn;
-                g_i[tid] = r.i;
-                g_j[tid] = r.j;
-            }
-            if (tid == 0) grp_lo = int(hi - len);
+    for (int64_t hi = Vst ? 0 : cnt; hi > 0;) {
+        const int64_t lo = hi > kChunk ? hi - kChunk : 0;
+        const int len = int(hi - lo);
+        for (int e = tid; e < len; e += blockDim.x) {
+            const lsvd_rotor r = rot[lo + e];
+            double sn, cs;
+            sincos(r.theta, &sn, &cs);
+            g_cs[e] = make_double2(cs, sn);
+            g_ij[e] = int(r.i) | (int(r.j) << 16);
         }
+        // groups of four entries of one round are disjoint: replayed with all
+        // loads first (the stream is in round order)
+        for (int g = tid; g < len / 4; g += blockDim.x)
+            g_safe[g] = rot[lo + 4 * g].round == rot[lo + 4 * g + 3].round;
         __syncthreads();
-        const int lo = grp_lo;
-        const int nr = int(hi - lo);
-        for (int e = tid; e < nr * n; e += blockDim.x) {
-            const int q = e / n, col = e % n;
-            const double c = g_c[q], sn = g_s[q];
-            const int ri = g_i[q], rj = g_j[q];
-            const double xi = V[ri * ld + col], xj = V[rj * ld + col];
-            V[ri * ld + col] = c * xi + sn * xj;
-            V[rj * ld + col] = -sn * xi + c * xj;
+        if (tid < n) {
+            const int col = tid;
+            auto one = [&](int e) {
+                const double2 cs = g_cs[e];
+                const int ij = g_ij[e];
+                const int ri = ij & 0xffff, rj = ij >> 16;
+                const double xi = V[ri * ld + col], xj = V[rj * ld + col];
+                V[ri * ld + col] = cs.x * xi + cs.y * xj;
+                V[rj * ld + col] = -cs.y * xi + cs.x * xj;
+            };
+            const int ng = len / 4;
+            for (int e = len - 1; e >= 4 * ng; --e) one(e);
+            for (int gi = ng - 1; gi >= 0; --gi) {
+                const int e0 = 4 * gi;
+                if (g_safe[gi]) {
+                    int ri[4], rj[4];
+                    double2 cs[4];
+                    double xi[4], xj[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        cs[u] = g_cs[e0 + u];
+                        const int ij = g_ij[e0 + u];
+                        ri[u] = ij & 0xffff;
+                        rj[u] = ij >> 16;
+                        xi[u] = V[ri[u] * ld + col];
+                        xj[u] = V[rj[u] * ld + col];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        V[ri[u] * ld + col] = cs[u].x * xi[u] + cs[u].y * xj[u];
+                        V[rj[u] * ld + col] = -cs[u].y * xi[u] + cs[u].x * xj[u];
+                    }
+                } else {
+                    one(e0 + 3);
+                    one(e0 + 2);
+                    one(e0 + 1);
+                    one(e0);
+                }
+            }
         }
         __syncthreads();
         hi = lo;
