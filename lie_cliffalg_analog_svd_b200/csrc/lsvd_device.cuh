@@ -700,7 +700,7 @@ __device__ inline int jacobi2pp_sweeps(const Team& t, int n, double* B0, double*
 
 // Blocked two-sided Jacobi for the same eigensolve (eigh_jacobi_full,
 // src/lie_svd_small.rs:212-285), used when no rotor stream is requested.
-// Indices are cut into blocks of B (8 for n >= 40, else 4) and the blocks
+// Indices are cut into blocks of B (8 for n >= 45, else 4) and the blocks
 // are paired by the circle method; in block layer l every block pair k owns
 // 2B indices.  One warp solves the 2B x 2B principal sub-block S_k of its
 // block pair: B rounds of B disjoint rotations (cross pairs; at layer 0 also
@@ -714,8 +714,17 @@ __device__ inline int jacobi2pp_sweeps(const Team& t, int n, double* B0, double*
 // once per rotation layer, and R is applied with 2B FMAs per load.
 // P: natural order, column-major, leading dimension pld; scr: scratch of
 // nbp * 2 * (2B)^2 doubles.  Returns the sweeps started.
+// Smallest n for the blocked sweep (where it overtakes the layer-by-layer
+// sweep on B200; a build may override it).
+#ifndef LSVD_BLOCK_JACOBI_MIN_N
+#define LSVD_BLOCK_JACOBI_MIN_N 33
+#endif
+
+// Block size: 8 from n = 45 (the scratch of n = 40..44 is too small for it), else 4.
+__host__ __device__ constexpr int block_jacobi_b(int n) { return n >= 45 ? 8 : 4; }
+
 __device__ inline int block_jacobi_fits(int n, int scr_doubles) {
-    const int B = n >= 40 ? 8 : 4, B2 = 2 * B;
+    const int B = block_jacobi_b(n), B2 = 2 * B;
     const int nbl = (n + B - 1) / B, nbe = nbl + (nbl & 1);
     // sub-blocks S, R per block pair, then the block-pair table (64 ints) and the
     // per-warp rotation tables (8 ints + 16 double2 per warp, 8 warps)
@@ -951,7 +960,7 @@ __device__ inline int jacobi_block_sweeps_t(const Team& t, int n, double* P, int
 __device__ inline int jacobi_block_sweeps(const Team& t, int n, double* P, int pld, double* scr,
                                           double* V, int ldv, double ref_norm, int max_sweeps,
                                           TeamScratch* sc, long long* rotations, bool* capped) {
-    if (n >= 40)
+    if (block_jacobi_b(n) == 8)
         return jacobi_block_sweeps_t<8>(t, n, P, pld, scr, V, ldv, ref_norm, max_sweeps, sc, rotations, capped);
     return jacobi_block_sweeps_t<4>(t, n, P, pld, scr, V, ldv, ref_norm, max_sweeps, sc, rotations, capped);
 }
@@ -1091,11 +1100,11 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     // of the ping-pong buffer Vb (leading dimension m); Q is parked in the U
     // output (global) so that Q's buffer can be the second ping-pong buffer.
     const int m = (n % 2 == 0) ? n : n + 1;
-    // Without a rotor stream to record, n >= 48 takes the blocked sweep (P in
-    // natural order, odd leading dimension m + 1); otherwise the layer-by-
-    // layer sweep with P in pair-position order (leading dimension m).  The
-    // threshold is where the blocked sweep overtakes (measured on B200).
-    const bool blocked = job.rotors == nullptr && n >= 48 && block_jacobi_fits(n, ld * np);
+    // Without a rotor stream to record, n >= LSVD_BLOCK_JACOBI_MIN_N takes the
+    // blocked sweep (P in natural order, odd leading dimension m + 1);
+    // otherwise the layer-by-layer sweep with P in pair-position order
+    // (leading dimension m).
+    const bool blocked = job.rotors == nullptr && n >= LSVD_BLOCK_JACOBI_MIN_N && block_jacobi_fits(n, ld * np);
     const int pstride = blocked ? m + 1 : m;
     for (int x = t.tid; x < m; x += t.nthreads) {
         // layer 0: pair k = (m-1, 0) for k = 0, else (k, m-1-k) in ring m-1
