@@ -210,11 +210,23 @@ LSVD_API lsvd_joint_params lsvd_joint_params_for_n(int64_t n);
  * M: families x K matrices of n x n, back to back (row-major); V: families x
  * n x n (the shared basis, columns = joint eigenvectors); diag: families x K
  * x n (the diagonals of V^T M_k V); traces: `families` entries, HOST memory
- * always.  params NULL = lsvd_joint_params_for_n(n).  K in 1..99. */
+ * always.  params NULL = lsvd_joint_params_for_n(n).  K in 1..93. */
 LSVD_API lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, int64_t K, int64_t n,
                                        const double* M, const lsvd_joint_params* params,
                                        double* V, double* diag, lsvd_joint_trace* traces,
                                        uint32_t flags);
+
+/* Replaces LieSvdJoint::joint_svd_with_params (src/lie_svd_joint.rs:170-261)
+ * for `families` independent families at once.  M: families x K matrices of
+ * rows x cols, back to back (row-major); U: families x rows x rows (left
+ * basis); sig: families x K x min(rows, cols) (|diag| of U^T M_k V, the
+ * reference's diagonal_corridor); Vt: families x cols x cols; traces: HOST
+ * memory always.  params NULL = lsvd_joint_params_for_n(min(rows, cols)).
+ * K <= 90 and max(rows, cols) up to ~500 (shared memory). */
+LSVD_API lsvd_status lsvd_joint_svd_f64(lsvd_context* ctx, int64_t families, int64_t K, int64_t rows,
+                                        int64_t cols, const double* M, const lsvd_joint_params* params,
+                                        double* U, double* sig, double* Vt, lsvd_joint_trace* traces,
+                                        uint32_t flags);
 
 /* ------------------------------------------------ large polar factor ---- */
 /* Polar factor Q (m x n, Q^T Q = I) of a large dense A (m >= n) by the

@@ -85,6 +85,7 @@ SIGNATURES = {
     "lsvd_svd_batched_noalloc_f64": (C.c_int, [P, I64, P, P, P, P, P, P, U32]),
     "lsvd_joint_params_for_n": (JointParams, [I64]),
     "lsvd_jade_sym_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, U32]),
+    "lsvd_joint_svd_f64": (C.c_int, [P, I64, I64, I64, I64, P, P, P, P, P, P, U32]),
     "lsvd_polar_f64": (C.c_int, [P, I64, I64, P, I64, P, I64, C.c_int, P, U32]),
     "lsvd_gemm_nt_lowp": (C.c_int, [P, I64, I64, I64, P, P, P, C.c_int]),
     "lsvd_svd_batched_stream_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, I64, P, P, P, U32]),

@@ -354,8 +354,29 @@ class JointDiagonalizationTrace:
 
 
 class LieSvdJoint:
-    """``LieSvdJoint`` symmetric route (src/lie_svd_joint.rs:61-158) on the GPU,
-    plus a batched form over independent families."""
+    """``LieSvdJoint`` (src/lie_svd_joint.rs:61-261) on the GPU: the symmetric
+    Phase-JADE route and the two-sided joint SVD, each also batched over
+    independent families."""
+
+    @staticmethod
+    def joint_svd(matrices, ctx: Context | None = None):
+        """``joint_svd`` (src/lie_svd_joint.rs:163): (U, per-matrix |diagonals|,
+        Vt, trace) with ``JointDiagonalizationParams::for_n(min(rows, cols))``."""
+        return _joint_svd(matrices, None, ctx)
+
+    @staticmethod
+    def joint_svd_with_params(matrices, params: "JointDiagonalizationParams",
+                              ctx: Context | None = None):
+        """``joint_svd_with_params`` (src/lie_svd_joint.rs:170-261)."""
+        return _joint_svd(matrices, params, ctx)
+
+    @staticmethod
+    def joint_svd_families(m, params: "JointDiagonalizationParams | None" = None,
+                           ctx: Context | None = None):
+        """``m``: (families, K, rows, cols).  Returns U (families, rows, rows),
+        |diagonals| (families, K, min(rows, cols)), Vt (families, cols, cols) and
+        one trace per family."""
+        return _joint_svd_families(m, params, ctx)
 
     @staticmethod
     def diagonalize_symmetric(matrices, ctx: Context | None = None):
@@ -396,6 +417,33 @@ class LieSvdJoint:
         traces = [JointDiagonalizationTrace(t.initial_offdiag, t.final_offdiag, t.sweeps,
                                             t.rotations, t.rejected_rotations) for t in tr]
         return v, d, traces
+
+
+def _joint_svd_families(m, params, ctx):
+    ctx = ctx or default_context()
+    m = _f64(m)
+    F, K, r, c = m.shape
+    kk = min(r, c)
+    u = np.empty((F, r, r)); s = np.empty((F, K, kk)); vt = np.empty((F, c, c))
+    tr = (L.JointTrace * F)()
+    p = None
+    if params is not None:
+        p = L.JointParams(params.max_sweeps, params.tol, params.min_pair_scale, params.line_search_steps)
+    st = ctx.lib.lsvd_joint_svd_f64(ctx.handle, F, K, r, c, _ptr(m), C.byref(p) if p else None,
+                                    _ptr(u), _ptr(s), _ptr(vt), tr, 0)
+    _check(ctx.lib, ctx.handle, st, "LieSvdJoint::joint_svd")
+    traces = [JointDiagonalizationTrace(t.initial_offdiag, t.final_offdiag, t.sweeps, t.rotations,
+                                        t.rejected_rotations) for t in tr]
+    return u, s, vt, traces
+
+
+def _joint_svd(matrices, params=None, ctx=None):
+    mats = [_f64(x) for x in matrices]
+    if not mats:
+        raise L.LsvdError(L.BAD_SHAPE, "LieSvdJoint::joint_svd: empty matrix set")
+    m = np.stack(mats)[None]
+    u, s, vt, traces = _joint_svd_families(m, params, ctx)
+    return u[0], [s[0, k].copy() for k in range(s.shape[1])], vt[0], traces[0]
 
 
 class PolarResult:

@@ -39,39 +39,11 @@
 
 #include "lsvd.h"
 #include "lsvd_internal.h"
+#include "lsvd_joint_common.cuh"
 
 namespace {
 
-constexpr int B = 8;        // block size
-constexpr int B2 = 2 * B;   // indices of a block pair
-// Shared sub-block layout of the solve kernel: row stride B2 + 1 and matrix
-// stride B2 (B2 + 1) + 1 doubles, so that lanes walking a column, or the same
-// entry of consecutive matrices, fall in different banks.
-constexpr int SLD = B2 + 1, MST = B2 * SLD + 1;
-constexpr int kThreads = 256;
-constexpr double kPi = 3.141592653589793238462643383279502884;
-
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-__device__ __forceinline__ double wrap_quarter(double a) {  // wrap_jacobi_angle, :506-514
-    while (a > 0.25 * kPi) a -= 0.5 * kPi;
-    while (a < -0.25 * kPi) a += 0.5 * kPi;
-    return a;
-}
-
-__device__ __forceinline__ void rr_pair(int m, int layer, int k, int& a, int& b) {
-    const int ring = m - 1;
-    if (k == 0) {
-        a = m - 1;
-        b = layer % ring;
-    } else {
-        a = (layer + k) % ring;
-        b = (layer + ring - k) % ring;
-    }
-}
+using namespace lsvd::joint;
 
 struct JadeArgs {
     int F, K, n, nbe;        // families, matrices per family, order, blocks (even)
@@ -295,11 +267,6 @@ __global__ void __launch_bounds__(kThreads, 1) jade_solve_kernel(JadeArgs a) {
 // All R of the family sit in shared memory for the whole matrix, so M's data
 // cross HBM once per layer.  Positions past n are padding (R is the
 // identity there and they are never loaded or stored).
-__device__ __forceinline__ int jade_pos(int blk_lo, int blk_hi, int pos, int n) {
-    const int g = (pos < B ? blk_lo : blk_hi) * B + (pos % B);
-    return g < n ? g : -1;
-}
-
 __global__ void __launch_bounds__(kThreads, 2) jade_apply_kernel(JadeArgs a) {
     const int k = blockIdx.x, f = blockIdx.y;
     if (!a.active[f]) return;
@@ -330,7 +297,7 @@ __global__ void __launch_bounds__(kThreads, 2) jade_apply_kernel(JadeArgs a) {
             double x[B2];
 #pragma unroll
             for (int r = 0; r < B2; ++r) {
-                const int g = jade_pos(plo, phi, r, n);
+                const int g = block_pos(plo, phi, r, n);
                 x[r] = g >= 0 ? M[size_t(g) * n + col] : 0.0;
             }
             if (isV) {
@@ -361,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 2) jade_apply_kernel(JadeArgs a) {
                 double x0[B2], x1[B2];
 #pragma unroll
                 for (int c = 0; c < B2; ++c) {
-                    const int g = jade_pos(qlo, qhi, c, n);
+                    const int g = block_pos(qlo, qhi, c, n);
                     x0[c] = g >= 0 ? T[rr * ldt + g] : 0.0;
                     x1[c] = g >= 0 ? T[(rr + B) * ldt + g] : 0.0;
                 }
@@ -382,7 +349,7 @@ __global__ void __launch_bounds__(kThreads, 2) jade_apply_kernel(JadeArgs a) {
                 __syncwarp();  // every lane of the warp read its rows before any writes
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    const int g = jade_pos(qlo, qhi, c0 + u, n);
+                    const int g = block_pos(qlo, qhi, c0 + u, n);
                     if (g >= 0) {
                         T[rr * ldt + g] = y0[u];
                         T[(rr + B) * ldt + g] = y1[u];
@@ -396,7 +363,7 @@ __global__ void __launch_bounds__(kThreads, 2) jade_apply_kernel(JadeArgs a) {
         for (int col = tid; col < n; col += kThreads) {
 #pragma unroll
             for (int r = 0; r < B2; ++r) {
-                const int g = jade_pos(plo, phi, r, n);
+                const int g = block_pos(plo, phi, r, n);
                 if (g >= 0) {
                     const double v = T[r * ldt + col];
                     M[size_t(g) * n + col] = v;
