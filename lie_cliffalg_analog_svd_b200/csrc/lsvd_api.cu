@@ -101,6 +101,8 @@ lsvd_context::~lsvd_context() {
     for (auto* b : {&ws_a, &ws_u, &ws_s, &ws_vt, &ws_diag, &ws_misc, &ws_rot, &ws_polar})
         b->release();
     lsvd_destroy_blas(cublas);
+    if (h2d_stream) cudaStreamDestroy(h2d_stream);
+    if (d2h_stream) cudaStreamDestroy(d2h_stream);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -561,6 +563,133 @@ BatchPlan* lsvd_get_plan(lsvd_context* ctx, int64_t count, const int32_t* n, lsv
     return raw;
 }
 
+// Host-pointer batches of at least kPipeMin matrices are cut into kPipeChunks
+// contiguous chunks of equal cost (sum of n^3), each with its own plan and
+// staging buffers, so that the copies overlap the solves: H2D of every chunk
+// on one copy stream, the solves in order on the context stream, D2H of
+// chunk c on a second copy stream as soon as its solve is done.  The results
+// are those of the unchunked call (every matrix is solved independently).
+constexpr int64_t kPipeMin = 16384;
+constexpr int kPipeChunks = 4;
+
+static lsvd_status batched_pipelined(lsvd_context* ctx, int64_t count, const int32_t* n, const double* A,
+                                     double* U, double* S, double* Vt, lsvd_diag* diags,
+                                     lsvd_precision precision, bool want_diag) {
+    constexpr int C = kPipeChunks;
+    cudaError_t e = cudaSuccess;
+    if (!ctx->h2d_stream && (e = cudaStreamCreateWithFlags(&ctx->h2d_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "copy stream");
+    if (!ctx->d2h_stream && (e = cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "copy stream");
+    // cost-balanced cuts (every chunk non-empty) and the element offsets of every chunk
+    std::vector<double> pre(size_t(count) + 1, 0.0);
+    for (int64_t t = 0; t < count; ++t) pre[t + 1] = pre[t] + double(n[t]) * n[t] * n[t];
+    int64_t cut[C + 1];
+    cut[0] = 0;
+    for (int c = 1; c < C; ++c) {
+        const int64_t x = std::lower_bound(pre.begin(), pre.end(), pre[count] * c / C) - pre.begin();
+        cut[c] = std::min(std::max(x, cut[c - 1] + 1), count - (C - c));
+    }
+    cut[C] = count;
+    int64_t aoff[C + 1], soff[C + 1];
+    {
+        int64_t a = 0, s = 0, t = 0;
+        for (int c = 0; c <= C; ++c) {
+            for (; t < cut[c]; ++t) {
+                a += int64_t(n[t]) * n[t];
+                s += n[t];
+            }
+            aoff[c] = a;
+            soff[c] = s;
+        }
+    }
+    // every plan stays valid while the chunks run: make room in the cache first
+    if (ctx->plans.size() + C > 16) ctx->plans.clear();
+    BatchPlan* plans[C];
+    for (int c = 0; c < C; ++c) {
+        lsvd_status st;
+        plans[c] = lsvd_get_plan(ctx, cut[c + 1] - cut[c], n + cut[c], precision, &st);
+        if (!plans[c]) return st;
+    }
+    cudaEvent_t ev[2 * C + 1];
+    int created = 0;
+    for (; created < 2 * C + 1; ++created)
+        if ((e = cudaEventCreateWithFlags(&ev[created], cudaEventDisableTiming)) != cudaSuccess) break;
+    auto destroy = [&]() {
+        for (int i = 0; i < created; ++i) cudaEventDestroy(ev[i]);
+    };
+    if (e != cudaSuccess) {
+        destroy();
+        return lsvd_ctx_cuda(ctx, e, "events");
+    }
+    cudaEvent_t ev_start = ev[2 * C];
+    lsvd_status out = LSVD_OK;
+    double *dA[C], *dU[C], *dS[C], *dV[C];
+    lsvd_diag* dD[C];
+    // the copy streams start after everything already queued on the context stream
+    if ((e = cudaEventRecord(ev_start, ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(ctx->h2d_stream, ev_start, 0)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(ctx->d2h_stream, ev_start, 0)) != cudaSuccess)
+        out = lsvd_ctx_cuda(ctx, e, "pipeline start");
+    for (int c = 0; c < C && out == LSVD_OK; ++c) {
+        BatchPlan& P = *plans[c];
+        const int64_t cnt = cut[c + 1] - cut[c];
+        dA[c] = static_cast<double*>(P.d_a.get(size_t(P.a_elems) * 8, &e));
+        if (e == cudaSuccess) dU[c] = static_cast<double*>(P.d_u.get(size_t(P.a_elems) * 8, &e));
+        if (e == cudaSuccess) dS[c] = static_cast<double*>(P.d_s.get(size_t(P.s_elems) * 8, &e));
+        if (e == cudaSuccess) dV[c] = static_cast<double*>(P.d_vt.get(size_t(P.a_elems) * 8, &e));
+        dD[c] = nullptr;
+        if (e == cudaSuccess && diags)
+            dD[c] = static_cast<lsvd_diag*>(P.d_diag.get(size_t(cnt) * sizeof(lsvd_diag), &e));
+        if (e != cudaSuccess) {
+            out = lsvd_ctx_cuda(ctx, e, "batch buffers");
+            break;
+        }
+        if ((e = cudaMemcpyAsync(dA[c], A + aoff[c], size_t(P.a_elems) * 8, cudaMemcpyHostToDevice,
+                                 ctx->h2d_stream)) != cudaSuccess ||
+            (e = cudaEventRecord(ev[c], ctx->h2d_stream)) != cudaSuccess)
+            out = lsvd_ctx_cuda(ctx, e, "copy A");
+    }
+    for (int c = 0; c < C && out == LSVD_OK; ++c) {
+        BatchPlan& P = *plans[c];
+        const int64_t cnt = cut[c + 1] - cut[c];
+        if ((e = cudaStreamWaitEvent(ctx->stream, ev[c], 0)) != cudaSuccess) {
+            out = lsvd_ctx_cuda(ctx, e, "pipeline wait");
+            break;
+        }
+        if ((out = lsvd_run_plan(ctx, P, dA[c], dU[c], dS[c], dV[c], dD[c], want_diag, true)) != LSVD_OK) break;
+        cudaStream_t s = ctx->d2h_stream;
+        if ((e = cudaEventRecord(ev[C + c], ctx->stream)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(s, ev[C + c], 0)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(U + aoff[c], dU[c], size_t(P.a_elems) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(S + soff[c], dS[c], size_t(P.s_elems) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(Vt + aoff[c], dV[c], size_t(P.a_elems) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (diags && (e = cudaMemcpyAsync(diags + cut[c], dD[c], size_t(cnt) * sizeof(lsvd_diag),
+                                           cudaMemcpyDeviceToHost, s)) != cudaSuccess))
+            out = lsvd_ctx_cuda(ctx, e, "copy out");
+    }
+    // wait for all three streams, then the per-chunk outcome flags
+    if ((e = cudaStreamSynchronize(ctx->h2d_stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->d2h_stream)) != cudaSuccess) {
+        if (out == LSVD_OK) out = lsvd_ctx_cuda(ctx, e, "pipeline sync");
+    }
+    int agg = 0;
+    for (int c = 0; c < C && out == LSVD_OK; ++c) {
+        int a = 0;
+        if ((e = cudaMemcpy(&a, plans[c]->s_agg, 4, cudaMemcpyDeviceToHost)) != cudaSuccess) {
+            out = lsvd_ctx_cuda(ctx, e, "flags");
+            break;
+        }
+        agg |= a;
+    }
+    destroy();
+    if (out != LSVD_OK) return out;
+    if (agg & LSVD_MAT_NONFINITE) return LSVD_NONFINITE_INPUT;
+    if (agg & LSVD_MAT_JACOBI_CAP) return LSVD_NOT_CONVERGED;
+    return LSVD_OK;
+}
+
 extern "C" lsvd_status lsvd_svd_batched_f64(lsvd_context* ctx, int64_t count, const int32_t* n,
                                             const double* A, double* U, double* S, double* Vt,
                                             lsvd_diag* diags, lsvd_precision precision,
@@ -578,6 +707,8 @@ extern "C" lsvd_status lsvd_svd_batched_f64(lsvd_context* ctx, int64_t count, co
         precision != LSVD_PREC_MIXED_BF16)
         return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "unknown precision");
     cudaSetDevice(ctx->device);
+    if (!is_dev(flags) && count >= kPipeMin)
+        return batched_pipelined(ctx, count, n, A, U, S, Vt, diags, precision, (flags & LSVD_WANT_DIAG) != 0);
     lsvd_status st;
     BatchPlan* P = lsvd_get_plan(ctx, count, n, precision, &st);
     if (!P) return st;

@@ -87,6 +87,8 @@ struct lsvd_context {
     int64_t launches = 0;
     DeviceBuffer ws_a, ws_u, ws_s, ws_vt, ws_diag, ws_misc, ws_rot, ws_polar;
     void* cublas = nullptr;  // cublasHandle_t of the large-polar FP64 GEMMs, created on first use
+    // copy streams of the pipelined host-pointer batched path, created on first use
+    cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
     std::unordered_map<uint64_t, std::unique_ptr<BatchPlan>> plans;
     ~lsvd_context();
 };

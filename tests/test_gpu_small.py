@@ -345,3 +345,29 @@ def test_metrics_match_oracle():
     for f in ("rel_recon", "orth_u", "orth_v", "sigma_max_rel", "sigma_tail_rel"):
         x, y = getattr(mg, f), getattr(mo, f)
         assert abs(x - y) <= 1e-3 * abs(y) + 1e-18, f
+
+
+def test_batched_host_pipeline_matches_device():
+    # >= 16384 matrices from host memory take the chunked, copy-overlapped
+    # path; every matrix is solved independently, so the results must equal
+    # the device-pointer (single plan) call bit for bit
+    import torch
+    ns, a, sig = P.uneven_batch_workload(20000, seed=77, n_lo=2, n_hi=24)
+    pin = lambda k: torch.empty(k, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    a_h = pin(a.size)
+    a_h[:] = a
+    so = int(ns.astype(np.int64).sum())
+    out_h = (pin(a.size), pin(so), pin(a.size), np.empty(ns.size, dtype=L.DIAG_DTYPE))
+    u, s, vt, dg, st = svd_batched(ns, a_h, want_diag=True, out=out_h)
+    assert st == 0
+    ud, sd, vtd, dgd, std = svd_batched(ns, torch.from_numpy(a).cuda(), want_diag=True)
+    assert std == 0
+    assert np.array_equal(s, sd.cpu().numpy())
+    assert np.array_equal(u, ud.cpu().numpy()) and np.array_equal(vt, vtd.cpu().numpy())
+    dgd = np.frombuffer(dgd.cpu().numpy().tobytes(), dtype=L.DIAG_DTYPE)
+    assert np.array_equal(dg["rotations"], dgd["rotations"])
+    first = np.concatenate([[0], np.cumsum(ns)[:-1]])
+    assert np.max(np.abs(s - sig) / np.repeat(sig[first], ns)) <= 1e-13
+    # pageable host memory takes the same path (its copies are then synchronous)
+    u2, s2, vt2, _, st2 = svd_batched(ns, a)
+    assert st2 == 0 and np.array_equal(s2, s)
