@@ -206,14 +206,14 @@ EncodeFn encode_fn() {
     return fn;
 }
 
-// 2-D K-major map: rows x cols (cols = K contiguous), box 128 rows x 128 bytes.
-bool make_map(CUtensorMap* map, int prec, const void* ptr, int rows, int cols) {
+// 2-D K-major map: rows x cols (cols = K contiguous), box box_rows x 128 bytes.
+bool make_map(CUtensorMap* map, int prec, const void* ptr, int rows, int cols, int box_rows) {
     EncodeFn fn = encode_fn();
     if (!fn) return false;
     const int elem = prec == kBF16 ? 2 : 4;
     cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
     cuuint64_t strides[1] = {cuuint64_t(cols) * elem};
-    cuuint32_t box[2] = {cuuint32_t(kSliceBytes / elem), cuuint32_t(kTile)};
+    cuuint32_t box[2] = {cuuint32_t(kSliceBytes / elem), cuuint32_t(box_rows)};
     cuuint32_t es[2] = {1, 1};
     return fn(map, prec == kBF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
               const_cast<void*>(ptr), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -221,16 +221,25 @@ bool make_map(CUtensorMap* map, int prec, const void* ptr, int rows, int cols) {
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+template <int PREC, int TN>
+cudaError_t launch_gemm_t(cudaStream_t st, const void* A, const void* B, float* C, int M, int N, int K,
+                          int* err) {
+    CUtensorMap ma, mb;
+    if (!make_map(&ma, PREC, A, M, K, kTile) || !make_map(&mb, PREC, B, N, K, TN))
+        return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<PREC, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem_bytes(TN));
+    if (e != cudaSuccess) return e;
+    tc_gemm_kernel<PREC, TN><<<dim3(N / TN, M / kTile), 128, smem_bytes(TN), st>>>(ma, mb, C, N, K, err);
+    return cudaGetLastError();
+}
+
+// 128 x 256 tiles where N allows them (half the A traffic per flop), else 128 x 128.
 template <int PREC>
 cudaError_t launch_gemm(cudaStream_t st, const void* A, const void* B, float* C, int M, int N, int K,
                         int* err) {
-    CUtensorMap ma, mb;
-    if (!make_map(&ma, PREC, A, M, K) || !make_map(&mb, PREC, B, N, K)) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kSmemBytes);
-    if (e != cudaSuccess) return e;
-    tc_gemm_kernel<PREC><<<dim3(N / kTile, M / kTile), 128, kSmemBytes, st>>>(ma, mb, C, N, K, err);
-    return cudaGetLastError();
+    return N % 256 == 0 ? launch_gemm_t<PREC, 256>(st, A, B, C, M, N, K, err)
+                        : launch_gemm_t<PREC, kTile>(st, A, B, C, M, N, K, err);
 }
 
 cublasHandle_t blas(lsvd_context* ctx) {

@@ -3,10 +3,11 @@
 //   C[M x N] (FP32, row-major) = A[M x K] * B[N x K]^T
 //
 // A and B are K-major (row-major, K contiguous), BF16 or FP32-stored TF32.
-// One CTA computes a 128 x 128 tile: TMA (cp.async.bulk.tensor.2d, 128-byte
-// swizzle, no multicast) brings 128 x 128-byte K-slices of A and B into a
-// 4-stage shared-memory ring guarded by mbarriers; one elected thread issues
-// tcgen05.mma (cta_group::1, M = 128, N = 128, FP32 accumulator in 128 TMEM
+// One CTA computes a 128 x TN tile (TN = 256 where N allows it, else 128):
+// TMA (cp.async.bulk.tensor.2d, 128-byte swizzle, no multicast) brings
+// 128-byte K-slices of 128 rows of A and TN rows of B into a 4-stage
+// shared-memory ring guarded by mbarriers; one elected thread issues
+// tcgen05.mma (cta_group::1, M = 128, N = TN, FP32 accumulator in TN TMEM
 // columns) and releases each stage with tcgen05.commit; after the last
 // K-slice the four warps read their 32 TMEM lanes with tcgen05.ld and store
 // FP32 rows.  Every mbarrier wait is bounded: on timeout the kernel records
@@ -22,11 +23,12 @@
 namespace lsvd {
 namespace tc {
 
-constexpr int kTile = 128;
+constexpr int kTile = 128;                             // M of a tile (and the smallest N)
 constexpr int kStages = 4;
 constexpr int kSliceBytes = 128;                       // K bytes per stage row
-constexpr int kStageBytes = 2 * kTile * kSliceBytes;   // A and B slices
-constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
+// Stage: an A slice of 128 rows and a B slice of TN rows (TN = 128 or 256).
+__host__ __device__ constexpr int stage_bytes(int tn) { return (kTile + tn) * kSliceBytes; }
+__host__ __device__ constexpr int smem_bytes(int tn) { return kStages * stage_bytes(tn) + 1024 + 256; }
 constexpr unsigned kSpinLimit = 1u << 26;              // bounded mbarrier waits: polls
 constexpr uint64_t kWaitNs = 2000000000ull;           // ... and wall time (2 s)
 
@@ -92,16 +94,16 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
 }
 
 // Instruction descriptor: FP32 accumulator, A/B format (1 = BF16 under
-// kind::f16, 2 = TF32 under kind::tf32), K-major A and B, N = 128, M = 128.
-template <int PREC>
+// kind::f16, 2 = TF32 under kind::tf32), K-major A and B, N = TN, M = 128.
+template <int PREC, int TN>
 __host__ __device__ constexpr uint32_t instr_desc() {
     return (1u << 4) | ((PREC == kBF16 ? 1u : 2u) << 7) | ((PREC == kBF16 ? 1u : 2u) << 10) |
-           (uint32_t(kTile >> 3) << 17) | (uint32_t(kTile >> 4) << 24);
+           (uint32_t(TN >> 3) << 17) | (uint32_t(kTile >> 4) << 24);
 }
 
-template <int PREC>
+template <int PREC, int TN>
 __device__ __forceinline__ void mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
-    constexpr uint32_t idesc = instr_desc<PREC>();
+    constexpr uint32_t idesc = instr_desc<PREC, TN>();
     if (PREC == kBF16) {
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -122,8 +124,9 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
                  : "memory");
 }
 
-// grid (N/128, M/128), 128 threads.  err: set to a nonzero code on timeout.
-template <int PREC>
+// grid (N/TN, M/128), 128 threads.  err: set to a nonzero code on timeout.
+// mapB's box is TN rows high.
+template <int PREC, int TN>
 __global__ void __launch_bounds__(128, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                    float* __restrict__ C, int ldc, int K, int* err) {
@@ -136,7 +139,8 @@ __global__ void __launch_bounds__(128, 1)
     __shared__ uint32_t tmem_base;
     __shared__ int s_err;
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int m0 = blockIdx.y * kTile, n0 = blockIdx.x * kTile;
+    constexpr int kStageBytes = stage_bytes(TN);
+    const int m0 = blockIdx.y * kTile, n0 = blockIdx.x * TN;
     constexpr int elem = (PREC == kBF16) ? 2 : 4;
     constexpr int kslice = kSliceBytes / elem;       // K elements per stage
     constexpr int kmma = (PREC == kBF16) ? 16 : 8;   // K per tcgen05.mma
@@ -154,7 +158,7 @@ __global__ void __launch_bounds__(128, 1)
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_base)),
-                     "r"(kTile));
+                     "r"(TN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -198,7 +202,7 @@ __global__ void __launch_bounds__(128, 1)
             for (int k = 0; k < kslice / kmma; ++k) {
                 // advance 32 bytes along K inside the swizzle atom (16-byte units)
                 const uint64_t off = uint64_t((k * kmma * elem) >> 4);
-                mma<PREC>(tmem, da + off, db + off, (kb > 0 || k > 0) ? 1u : 0u);
+                mma<PREC, TN>(tmem, da + off, db + off, (kb > 0 || k > 0) ? 1u : 0u);
             }
             mma_commit(smem_u32(&empty[s]));
         }
@@ -213,7 +217,7 @@ __global__ void __launch_bounds__(128, 1)
         const int row = m0 + warp * 32 + lane;
         float* crow = C + size_t(row) * ldc + n0;
 #pragma unroll 1
-        for (int c0 = 0; c0 < kTile; c0 += 32) {
+        for (int c0 = 0; c0 < TN; c0 += 32) {
             uint32_t v[32];
             const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0);
             asm volatile(
@@ -243,7 +247,7 @@ __global__ void __launch_bounds__(128, 1)
     __syncthreads();
     if (threadIdx.x == 0 && (s_err || !ok)) atomicExch(err, s_err ? s_err : 3);
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTile));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
 }
 
 }  // namespace tc

@@ -41,7 +41,8 @@ def _round_bf16(x: np.ndarray) -> np.ndarray:
 
 
 @pytest.mark.parametrize("prec", ["tf32", "bf16"])
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 512), (1024, 1024, 1024), (512, 128, 4096)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 512), (1024, 1024, 1024), (512, 128, 4096),
+                                   (128, 256, 64), (384, 768, 2048)])
 def test_tc_gemm(prec, M, N, K):
     import torch
     rng = np.random.default_rng(M * 7 + N * 3 + K)
