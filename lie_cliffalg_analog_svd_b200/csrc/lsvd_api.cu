@@ -156,7 +156,7 @@ static int variant_of(int ts, int g) { return (ts == 4 ? 3 : 0) + (g == 16 ? 1 :
 
 static cudaError_t launch_single(lsvd_context* ctx, const SmallJob& job) {
     const int n = job.n;
-    const size_t smem = size_t(team_smem_doubles(n)) * sizeof(double);
+    const size_t smem = size_t(team_smem_doubles(n, kCtaThreads / 32)) * sizeof(double);
     const bool big = n > 32;
     cudaError_t e;
     if (big) {
@@ -400,7 +400,7 @@ static lsvd_status build_plan(lsvd_context* ctx, int64_t count, const int32_t* n
         cfg.variant = variant_of(s.ts, s.g);
         const int lo = c == 0 ? 1 : kClassHi[c - 1] + 1;
         const int hi = kClassHi[c];
-        cfg.slice = !s.nwarps ? 0 : (prec == LSVD_PREC_FP64 ? team_smem_doubles(hi)
+        cfg.slice = !s.nwarps ? 0 : (prec == LSVD_PREC_FP64 ? team_smem_doubles(hi, s.nwarps)
                                                              : mixed_smem_doubles(hi));
         if (lo > hi) continue;
     }
@@ -494,7 +494,7 @@ static cudaError_t enqueue_plan(lsvd_context* ctx, BatchPlan& P, const double* A
     else
         batched_kernel<<<grid, kCtaThreads, smem, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    const int fsmem = team_smem_doubles(4) * 8;
+    const int fsmem = team_smem_doubles(4, kCtaThreads / 32) * 8;
     fallback_kernel<<<std::max(1, std::min(ctx->num_sms, int(P.count))), kCtaThreads, fsmem, st>>>(a);
     return cudaGetLastError();
 }

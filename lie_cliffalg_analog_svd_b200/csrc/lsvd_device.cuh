@@ -111,6 +111,63 @@ __device__ __forceinline__ void team_gemm(const Team& t, int np, int kdim, LA la
     }
 }
 
+// D += A B on one 8 x 8 tile: FP64 mma.sync m8n8k4.  Fragments (lane =
+// 4 g + q): a = A[g][q], b = B[q][g], d = D[g][2q], D[g][2q + 1].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// C[i][j] = sum_k A(k, i) B(k, j) for i, j < np (np a multiple of 8), the
+// same contract as team_gemm, on the FP64 tensor path: each warp owns a block
+// of 2 x wn 8 x 8 tiles (wn = ceil(np / 16) <= 4) and runs kdim rounded up to
+// 4 in k-steps of 4 (A and B must read zeros for k in [kdim, that)).  Every
+// lane calls epi for its two outputs of each tile it owns.
+template <class LA, class LB, class Epi>
+__device__ __forceinline__ void team_mma(const Team& t, int np, int kdim, LA la, LB lb, Epi epi) {
+    const int nt8 = np >> 3;
+    const int wn = (nt8 + 1) >> 1;
+    const int nblk = ((nt8 + 1) >> 1) * 2;
+    const int g = t.lane >> 2, q = t.lane & 3;
+    const int kd = (kdim + 3) & ~3;
+    for (int blk = t.warp; blk < nblk; blk += t.nwarps) {
+        const int ti0 = (blk >> 1) * 2, tj0 = (blk & 1) * wn;
+        bool vr[2], vc[4];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) vr[r] = ti0 + r < nt8;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) vc[c] = c < wn && tj0 + c < nt8;
+        double acc[2][4][2];
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[r][c][0] = acc[r][c][1] = 0.0;
+#pragma unroll 2
+        for (int k0 = 0; k0 < kd; k0 += 4) {
+            double a[2], b[4];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) a[r] = vr[r] ? la(k0 + q, (ti0 + r) * 8 + g) : 0.0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) b[c] = vc[c] ? lb(k0 + q, (tj0 + c) * 8 + g) : 0.0;
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (vc[c]) dmma_8x8x4(acc[r][c][0], acc[r][c][1], a[r], b[c]);
+        }
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (vr[r] && vc[c]) {
+                    const int i = (ti0 + r) * 8 + g, j = (tj0 + c) * 8 + 2 * q;
+                    epi(i, j, acc[r][c][0]);
+                    epi(i, j + 1, acc[r][c][1]);
+                }
+    }
+}
+
 // Pair k of round-robin layer `layer` over m (= n rounded up to even)
 // indices: the circle method of layer_pairs, src/lie_svd_joint.rs:524-539.
 __device__ __forceinline__ void rr_pair(int m, int layer, int k, int& a, int& b) {
@@ -299,9 +356,19 @@ struct alignas(16) TeamScratch {
 };
 
 __host__ __device__ constexpr int pad4(int n) { return (n + 3) & ~3; }
-// Doubles of shared memory one team needs for an n x n solve.
-__host__ __device__ constexpr int team_smem_doubles(int n) {
-    return 3 * (pad4(n) + 1) * pad4(n) + int(sizeof(TeamScratch) / sizeof(double));
+__host__ __device__ constexpr int pad8(int n) { return (n + 7) & ~7; }
+// Eight-warp teams with n > 32 run their products on the FP64 tensor path
+// (mma.sync m8n8k4, team_mma): buffers padded to 8 with leading dimension
+// np + 4 (= 4 mod 8, so that the 8 x 4 fragment loads of a half-warp hit 16
+// distinct banks).  Other teams use the scalar register-tiled team_gemm with
+// np = n rounded up to 4 and an odd leading dimension np + 1.
+__host__ __device__ constexpr bool team_uses_mma(int n, int nwarps) { return nwarps == 8 && n > 32; }
+__host__ __device__ constexpr int team_np(int n, bool mma) { return mma ? pad8(n) : pad4(n); }
+__host__ __device__ constexpr int team_ld(int n, bool mma) { return mma ? pad8(n) + 4 : pad4(n) + 1; }
+// Doubles of shared memory a team of `nwarps` warps needs for an n x n solve.
+__host__ __device__ constexpr int team_smem_doubles(int n, int nwarps) {
+    return 3 * team_ld(n, team_uses_mma(n, nwarps)) * team_np(n, team_uses_mma(n, nwarps)) +
+           int(sizeof(TeamScratch) / sizeof(double));
 }
 
 struct SmallJob {
@@ -726,9 +793,8 @@ __host__ __device__ constexpr int block_jacobi_b(int n) { return n >= 45 ? 8 : 4
 __device__ inline int block_jacobi_fits(int n, int scr_doubles) {
     const int B = block_jacobi_b(n), B2 = 2 * B;
     const int nbl = (n + B - 1) / B, nbe = nbl + (nbl & 1);
-    // sub-blocks S, R per block pair, then the block-pair table (64 ints) and the
-    // per-warp rotation tables (8 ints + 16 double2 per warp, 8 warps)
-    return (nbe / 2) * 2 * B2 * (B2 + 2) + 64 + 256 <= scr_doubles && nbe >= 2 && (nbe / 2) * B <= 32;
+    // sub-blocks S, R per block pair, then the block-pair table (64 ints)
+    return (nbe / 2) * 2 * B2 * (B2 + 2) + 32 <= scr_doubles && nbe >= 2 && (nbe / 2) * B <= 32;
 }
 
 // M[:, pair k columns] <- M[:, pair k columns] R_k for every block pair k of
@@ -774,9 +840,336 @@ __device__ __forceinline__ void seg_right_multiply(const Team& t, int n, int nbp
     }
 }
 
+// Pair j (0..B-1) of round rd of a block-pair solve over the 2B local indices:
+// rounds rd < B pair lo-block index j with hi-block index B + (j + rd) mod B
+// (every inter-block pair once); layer 0 adds B - 1 rounds that pair indices
+// inside each block (round-robin over B, pairs j < B/2 in the lo block).
+template <int B>
+__device__ __forceinline__ void bp_pair(int rd, int j, int& p, int& q) {
+    if (rd < B) {
+        p = j;
+        q = B + ((j + rd) & (B - 1));
+    } else {
+        int x, y;
+        rr_pair(B, rd - B, j & (B / 2 - 1), x, y);
+        const int o = j < B / 2 ? 0 : B;
+        p = o + min(x, y);
+        q = o + max(x, y);
+    }
+}
+
+// Rotation of pair (p, q) by the reference's rule (src/lie_svd_small.rs:
+// 235-249): tan(theta) = t with t the smaller root, the new diagonal
+// app - t apq, aqq + t apq.  Written in half-angle form so that the chain has
+// two reciprocal square roots and one reciprocal in place of a square root,
+// a division and a reciprocal square root:
+//   h = hypot(d, 2 apq), cos 2theta = |d| / h, sin 2theta = 2 apq / h,
+//   w = 1 + cos 2theta, cos theta = sqrt(w / 2), sin theta = sin 2theta / sqrt(2 w),
+//   |t| = sin 2theta / w.
+// Branch-free; expects the block scaled so that |entries| <= 1 (then
+// d^2 + 4 apq^2 cannot overflow; it is floored at the smallest normal).
+__device__ __forceinline__ void jacobi_rotation(double app, double aqq, double apq, double& c, double& s,
+                                                double& npp, double& nqq) {
+    const double d = aqq - app, g = 2.0 * apq;
+    // sign of t: that of theta = d / (2 apq), and + for theta = +-0 (the
+    // reference's theta >= 0 branch)
+    const double sg = d < 0.0 ? -1.0 : (d > 0.0 || g >= 0.0 ? 1.0 : -1.0);
+    const double x = fmax(fma(d, d, g * g), 2.2250738585072014e-308);
+    const double y = rsqrt(x);
+    const double w = fma(fabs(d), y, 1.0);
+    const double v = g * y;
+    const double z = rsqrt(2.0 * w);
+    const double rw = 1.0 / w;
+    c = w * z;
+    s = sg * (v * z);
+    const double ta = sg * (v * rw) * apq;
+    npp = app - ta;
+    nqq = aqq + ta;
+}
+
+// Two-sided Jacobi on one 2B x 2B sub-block S (stride B2 + 2) by one warp,
+// accumulating the rotations into R (R <- R J each round).  Lane j < B
+// computes pair j's rotation and writes pair j's 2 x 2 diagonal block (exact
+// new diagonal, zero off-diagonal); the rotations reach the other lanes by
+// shuffles.  Each lane owns whole 2 x 2 off-diagonal pair-blocks (row pair r,
+// column pair c) and applies both sides in registers:
+// S[{p_r,q_r}][{p_c,q_c}] <- J_r^T X J_c.
+// B = 8: pair-blocks (r, c0), (r, c0 + 4) and R rows {r, r + 8} x pairs {c0, c0 + 4};
+// B = 4: pair-block (r, c0) on lanes < 16 and R row lane & 7 x pair lane >> 3.
+// Returns the rotations this lane computed.
+template <int B, class Pairs>
+__device__ __forceinline__ int block_pair_round(int lane, int lo, int hi, int n, double thr, double* S, double* R,
+                                                Pairs pairs) {
+    constexpr int B2 = 2 * B, SLD = B2 + 2;
+    constexpr int NSB = B == 8 ? 2 : 1;  // S pair-blocks per lane
+    constexpr int NRI = B == 8 ? 4 : 1;  // R (row, pair) items per lane
+    constexpr unsigned FULL = 0xffffffffu;
+    const int r = lane & (B - 1);
+    int sc[NSB], rx[NRI], rc[NRI];
+    if constexpr (B == 8) {
+        sc[0] = lane >> 3;
+        sc[1] = (lane >> 3) + 4;
+        rx[0] = r; rc[0] = 0;
+        rx[1] = r; rc[1] = 1;
+        rx[2] = r + 8; rc[2] = 0;
+        rx[3] = r + 8; rc[3] = 1;
+    } else {
+        sc[0] = (lane >> 2) & 3;
+        rx[0] = lane & 7;
+        rc[0] = lane >> 3;
+    }
+    // ---- reads
+    int p, q;
+    pairs(r, p, q);  // lane j < B: its own pair j (r == lane there)
+    const int pr = p, qr = q;
+    double app = 0.0, aqq = 0.0, apq = 0.0;
+    if (lane < B) {
+        app = S[p * SLD + p];
+        aqq = S[q * SLD + q];
+        apq = S[p * SLD + q];
+    }
+    int pc[NSB], qc[NSB];
+    double xs[NSB][4];
+#pragma unroll
+    for (int u = 0; u < NSB; ++u) {
+        pairs(sc[u], pc[u], qc[u]);
+        xs[u][0] = S[pr * SLD + pc[u]];
+        xs[u][1] = S[pr * SLD + qc[u]];
+        xs[u][2] = S[qr * SLD + pc[u]];
+        xs[u][3] = S[qr * SLD + qc[u]];
+    }
+    int rpc[NRI], rqc[NRI];
+    double xr[NRI][2];
+#pragma unroll
+    for (int v = 0; v < NRI; ++v) {
+        if constexpr (B == 8) {
+            rpc[v] = pc[rc[v]];
+            rqc[v] = qc[rc[v]];
+        } else {
+            pairs(rc[v], rpc[v], rqc[v]);
+        }
+        xr[v][0] = R[rx[v] * SLD + rpc[v]];
+        xr[v][1] = R[rx[v] * SLD + rqc[v]];
+    }
+    // ---- pair `lane`'s rotation
+    double c = 1.0, s = 0.0, npp = app, nqq = aqq;
+    int nrot = 0;
+    bool rot = false;
+    if (lane < B) {
+        const int gp = (p < B ? lo : hi - B) + p, gq = (q < B ? lo : hi - B) + q;
+        if (gp < n && gq < n && fabs(apq) >= thr && apq != 0.0) {  // :232
+            jacobi_rotation(app, aqq, apq, c, s, npp, nqq);
+            rot = true;
+            nrot = 1;
+        }
+    }
+    const double cr = __shfl_sync(FULL, c, r), sr = __shfl_sync(FULL, s, r);
+    double cc[NSB], ss[NSB];
+#pragma unroll
+    for (int u = 0; u < NSB; ++u) {
+        cc[u] = __shfl_sync(FULL, c, sc[u]);
+        ss[u] = __shfl_sync(FULL, s, sc[u]);
+    }
+    double rcc[NRI], rss[NRI];
+#pragma unroll
+    for (int v = 0; v < NRI; ++v) {
+        if constexpr (B == 8) {
+            rcc[v] = cc[rc[v]];
+            rss[v] = ss[rc[v]];
+        } else {
+            rcc[v] = __shfl_sync(FULL, c, rc[v]);
+            rss[v] = __shfl_sync(FULL, s, rc[v]);
+        }
+    }
+    __syncwarp();  // every lane has read this round's S and R
+    // ---- writes
+    if (B == 8 || lane < 16) {
+#pragma unroll
+        for (int u = 0; u < NSB; ++u) {
+            if (sc[u] != r) {
+                // rows (p_r, q_r), then columns (p_c, q_c)
+                const double y00 = cr * xs[u][0] - sr * xs[u][2], y10 = sr * xs[u][0] + cr * xs[u][2];
+                const double y01 = cr * xs[u][1] - sr * xs[u][3], y11 = sr * xs[u][1] + cr * xs[u][3];
+                S[pr * SLD + pc[u]] = cc[u] * y00 - ss[u] * y01;
+                S[pr * SLD + qc[u]] = ss[u] * y00 + cc[u] * y01;
+                S[qr * SLD + pc[u]] = cc[u] * y10 - ss[u] * y11;
+                S[qr * SLD + qc[u]] = ss[u] * y10 + cc[u] * y11;
+            }
+        }
+    }
+    if (rot) {
+        S[p * SLD + p] = npp;
+        S[p * SLD + q] = 0.0;
+        S[q * SLD + p] = 0.0;
+        S[q * SLD + q] = nqq;
+    }
+#pragma unroll
+    for (int v = 0; v < NRI; ++v) {
+        R[rx[v] * SLD + rpc[v]] = rcc[v] * xr[v][0] - rss[v] * xr[v][1];
+        R[rx[v] * SLD + rqc[v]] = rss[v] * xr[v][0] + rcc[v] * xr[v][1];
+    }
+    __syncwarp();
+    return nrot;
+}
+
+// The B inter-block rounds of a block-pair solve (pair j of round rd is
+// (j, B + (j + rd) mod B)), software-pipelined across rounds.  Every lane
+// computes the rotation of its row pair r = lane mod B itself (lanes with the
+// same r agree bit for bit), so the rotation of round rd + 1 starts as soon as
+// round rd's values are in registers: its a_pp is pair r's new diagonal, its
+// a_qq pair r + 1's, and its a_pq the (p_r, q_{r+1}) entry of pair-block
+// (r, r + 1) after round rd, taken from the lane that owns that block.  The
+// shared-memory stores and loads of the pair-blocks overlap that chain (the
+// rounds are unrolled and branch-free).  Lane roles as in block_pair_round.
+// Returns the rotations of lanes < B.
+template <int B>
+__device__ __forceinline__ int inter_rounds(int lane, int lo, int hi, int n, double thr, double* S, double* R) {
+    constexpr int B2 = 2 * B, SLD = B2 + 2;
+    constexpr int NSB = B == 8 ? 2 : 1;
+    constexpr int NRI = B == 8 ? 4 : 1;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int r = lane & (B - 1), r1 = (r + 1) & (B - 1);
+    int sc[NSB], rx[NRI], rc[NRI];
+    int owner;  // lane owning pair-block (r, r + 1); it sits in slot r1 >> 2 there (B = 8)
+    if constexpr (B == 8) {
+        sc[0] = lane >> 3;
+        sc[1] = (lane >> 3) + 4;
+        rx[0] = r; rc[0] = 0;
+        rx[1] = r; rc[1] = 1;
+        rx[2] = r + 8; rc[2] = 0;
+        rx[3] = r + 8; rc[3] = 1;
+        owner = r + 8 * (r1 & 3);
+    } else {
+        sc[0] = (lane >> 2) & 3;
+        rx[0] = lane & 7;
+        rc[0] = lane >> 3;
+        owner = r + 4 * r1;
+    }
+    const bool s_writer = B == 8 || lane < 16;
+    const bool p_ok = lo + r < n;
+    // round 0 from shared memory
+    double app = S[r * SLD + r], aqq = S[(B + r) * SLD + B + r], apq = S[r * SLD + B + r];
+    double c, s, npp, nqq;
+    bool rot = p_ok && hi + r < n && fabs(apq) >= thr && apq != 0.0;  // :232
+    jacobi_rotation(app, aqq, apq, c, s, npp, nqq);
+    c = rot ? c : 1.0;
+    s = rot ? s : 0.0;
+    npp = rot ? npp : app;
+    nqq = rot ? nqq : aqq;
+    int nrot = 0;
+#pragma unroll
+    for (int rd = 0; rd < B; ++rd) {
+        const int qr = B + ((r + rd) & (B - 1));
+        int qc[NSB];
+        double xs[NSB][4];
+#pragma unroll
+        for (int u = 0; u < NSB; ++u) {
+            qc[u] = B + ((sc[u] + rd) & (B - 1));
+            xs[u][0] = S[r * SLD + sc[u]];
+            xs[u][1] = S[r * SLD + qc[u]];
+            xs[u][2] = S[qr * SLD + sc[u]];
+            xs[u][3] = S[qr * SLD + qc[u]];
+        }
+        int rpc[NRI], rqc[NRI];
+        double xr[NRI][2];
+#pragma unroll
+        for (int v = 0; v < NRI; ++v) {
+            if constexpr (B == 8) {
+                rpc[v] = sc[rc[v]];
+                rqc[v] = qc[rc[v]];
+            } else {
+                rpc[v] = rc[v];
+                rqc[v] = B + ((rc[v] + rd) & (B - 1));
+            }
+            xr[v][0] = R[rx[v] * SLD + rpc[v]];
+            xr[v][1] = R[rx[v] * SLD + rqc[v]];
+        }
+        nrot += (rot && lane < B) ? 1 : 0;
+        double cc[NSB], ss[NSB];
+#pragma unroll
+        for (int u = 0; u < NSB; ++u) {
+            cc[u] = __shfl_sync(FULL, c, sc[u]);
+            ss[u] = __shfl_sync(FULL, s, sc[u]);
+        }
+        double z[NSB][4];
+#pragma unroll
+        for (int u = 0; u < NSB; ++u) {
+            // rows (p_r, q_r), then columns (p_c, q_c); the diagonal pair-block
+            // takes the exact new diagonal and a zero off-diagonal (:244-249)
+            const double y00 = c * xs[u][0] - s * xs[u][2], y10 = s * xs[u][0] + c * xs[u][2];
+            const double y01 = c * xs[u][1] - s * xs[u][3], y11 = s * xs[u][1] + c * xs[u][3];
+            const bool dg = sc[u] == r, dr = dg && rot;
+            z[u][0] = dr ? npp : (dg ? xs[u][0] : cc[u] * y00 - ss[u] * y01);
+            z[u][1] = dr ? 0.0 : (dg ? xs[u][1] : ss[u] * y00 + cc[u] * y01);
+            z[u][2] = dr ? 0.0 : (dg ? xs[u][2] : cc[u] * y10 - ss[u] * y11);
+            z[u][3] = dr ? nqq : (dg ? xs[u][3] : ss[u] * y10 + cc[u] * y11);
+        }
+        double zr[NRI][2];
+#pragma unroll
+        for (int v = 0; v < NRI; ++v) {
+            double rcv, rsv;
+            if constexpr (B == 8) {
+                rcv = cc[rc[v]];
+                rsv = ss[rc[v]];
+            } else {
+                rcv = __shfl_sync(FULL, c, rc[v]);
+                rsv = __shfl_sync(FULL, s, rc[v]);
+            }
+            zr[v][0] = rcv * xr[v][0] - rsv * xr[v][1];
+            zr[v][1] = rsv * xr[v][0] + rcv * xr[v][1];
+        }
+        if (rd + 1 < B) {
+            // next round's rotation of pair r, from registers
+            double pz = z[0][1];
+            if constexpr (B == 8) pz = (r1 >> 2) ? z[1][1] : z[0][1];
+            const double apq_n = __shfl_sync(FULL, pz, owner);
+            const double aqq_n = __shfl_sync(FULL, nqq, r1);
+            const double app_n = npp;
+            rot = p_ok && hi + ((r + rd + 1) & (B - 1)) < n && fabs(apq_n) >= thr && apq_n != 0.0;
+            jacobi_rotation(app_n, aqq_n, apq_n, c, s, npp, nqq);
+            c = rot ? c : 1.0;
+            s = rot ? s : 0.0;
+            npp = rot ? npp : app_n;
+            nqq = rot ? nqq : aqq_n;
+        }
+        __syncwarp();  // every lane has read this round's S and R
+        if (s_writer) {
+#pragma unroll
+            for (int u = 0; u < NSB; ++u) {
+                S[r * SLD + sc[u]] = z[u][0];
+                S[r * SLD + qc[u]] = z[u][1];
+                S[qr * SLD + sc[u]] = z[u][2];
+                S[qr * SLD + qc[u]] = z[u][3];
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NRI; ++v) {
+            R[rx[v] * SLD + rpc[v]] = zr[v][0];
+            R[rx[v] * SLD + rqc[v]] = zr[v][1];
+        }
+        __syncwarp();
+    }
+    return nrot;
+}
+
+// One block-pair solve: B rounds over the inter-block pairs (j, B + (j + rd)
+// mod B), then on layer 0 the B - 1 round-robin rounds inside each block.
+template <int B>
+__device__ __forceinline__ int solve_block_pair(int lane, int layer, int lo, int hi, int n, double thr, double* S,
+                                                double* R) {
+    int nrot = inter_rounds<B>(lane, lo, hi, n, thr, S, R);
+    if (layer == 0) {
+#pragma unroll 1
+        for (int rd = B; rd < 2 * B - 1; ++rd)
+            nrot += block_pair_round<B>(lane, lo, hi, n, thr, S, R,
+                                        [rd](int j, int& p, int& q) { bp_pair<B>(rd, j, p, q); });
+    }
+    return nrot;
+}
+
 template <int B>
 __device__ inline int jacobi_block_sweeps_t(const Team& t, int n, double* P, int pld, double* scr,
-                                            double* V, int ldv, double ref_norm, int max_sweeps,
+                                            double* V, int ldv, double ref_norm, double thr, int max_sweeps,
                                             TeamScratch* sc, long long* rotations, bool* capped) {
     constexpr int B2 = 2 * B, SLD = B2 + 2, BB = B2 * SLD;  // sub-block stride B2 + 2: conflict-free columns
     const int nbl = (n + B - 1) / B, nbe = nbl + (nbl & 1), nbp = nbe / 2, layers = nbe - 1;
@@ -818,87 +1211,7 @@ __device__ inline int jacobi_block_sweeps_t(const Team& t, int n, double* P, int
                     R[r * SLD + c] = (r == c) ? 1.0 : 0.0;
                 }
                 __syncwarp();
-                const int rounds = B + (l == 0 ? B - 1 : 0);
-                for (int rd = 0; rd < rounds; ++rd) {
-                    const int lr = lane % B;
-                    int p, q;
-                    if (rd < B) {
-                        p = lr;
-                        q = B + (lr + rd) % B;
-                    } else {
-                        int x, y;
-                        rr_pair(B, rd - B, lr % (B / 2), x, y);
-                        const int o = lr < B / 2 ? 0 : B;
-                        p = o + min(x, y);
-                        q = o + max(x, y);
-                    }
-                    const int gp = (p < B ? lo : hi - B) + p, gq = (q < B ? lo : hi - B) + q;
-                    double c = 1.0, s = 0.0, npp = 0.0, nqq = 0.0;
-                    if (lane < B && gp < n && gq < n) {
-                        const double app = S[p * SLD + p], aqq = S[q * SLD + q], apq = S[p * SLD + q];
-                        npp = app;
-                        nqq = aqq;
-                        if (fabs(apq) >= 1e-300) {  // :232
-                            const double dd = aqq - app, g2 = 2.0 * apq;
-                            const double t0 = g2 / (fabs(dd) + sqrt(fma(dd, dd, g2 * g2)));
-                            const double tt = dd < 0.0 ? -t0 : t0;
-                            c = rsqrt(fma(tt, tt, 1.0));
-                            s = tt * c;
-                            npp = app - tt * apq;  // :244-249
-                            nqq = aqq + tt * apq;
-                            nrot++;
-                        }
-                    }
-                    // this round's rotations to a per-warp table (lanes < B), read
-                    // back by broadcast: rot_pq = p | q << 8, rot_cs = (c, s),
-                    // rot_nd = exact new diagonal (npp, nqq)
-                    int* rot_pq = bp_lo + 64 + t.warp * 8;
-                    double2* rot_cs = reinterpret_cast<double2*>(scr + nbp * 2 * BB + 64) + t.warp * 16;
-                    double2* rot_nd = rot_cs + 8;
-                    if (lane < B) {
-                        rot_pq[lane] = (s != 0.0) ? (p | (q << 8)) : -1;
-                        rot_cs[lane] = make_double2(c, s);
-                        rot_nd[lane] = make_double2(npp, nqq);
-                    }
-                    __syncwarp();
-                    // rows p, q of S: lane = (column, parity of the rotation index)
-                    {
-                        const int col = lane % B2;
-#pragma unroll
-                        for (int r = lane / B2; r < B; r += 32 / B2) {
-                            const int pq = rot_pq[r];
-                            if (pq < 0) continue;
-                            const int pr = pq & 255, qr = pq >> 8;
-                            const double2 cs = rot_cs[r];
-                            const double xv = S[pr * SLD + col], yv = S[qr * SLD + col];
-                            S[pr * SLD + col] = cs.x * xv - cs.y * yv;
-                            S[qr * SLD + col] = cs.y * xv + cs.x * yv;
-                        }
-                    }
-                    __syncwarp();
-                    // columns p, q of S and R: lane = (matrix, row)
-                    if (lane < 2 * B2) {
-                        const int mat = lane / B2, x = lane % B2;
-                        double* M = mat ? R : S;
-#pragma unroll
-                        for (int r = 0; r < B; ++r) {
-                            const int pq = rot_pq[r];
-                            if (pq < 0) continue;
-                            const int pr = pq & 255, qr = pq >> 8;
-                            const double2 cs = rot_cs[r];
-                            const double xv = M[x * SLD + pr], yv = M[x * SLD + qr];
-                            double vp = cs.x * xv - cs.y * yv, vq = cs.y * xv + cs.x * yv;
-                            if (!mat && (x == pr || x == qr)) {
-                                const double2 nd = rot_nd[r];
-                                vp = x == pr ? nd.x : 0.0;
-                                vq = x == pr ? 0.0 : nd.y;
-                            }
-                            M[x * SLD + pr] = vp;
-                            M[x * SLD + qr] = vq;
-                        }
-                    }
-                    __syncwarp();
-                }
+                nrot += solve_block_pair<B>(lane, l, lo, hi, n, thr, S, R);
             }
             t.sync();
             // ---- apply, pass 1: W = P R and V <- V R, one (row, block pair) segment per item
@@ -958,11 +1271,11 @@ __device__ inline int jacobi_block_sweeps_t(const Team& t, int n, double* P, int
 }
 
 __device__ inline int jacobi_block_sweeps(const Team& t, int n, double* P, int pld, double* scr,
-                                          double* V, int ldv, double ref_norm, int max_sweeps,
+                                          double* V, int ldv, double ref_norm, double thr, int max_sweeps,
                                           TeamScratch* sc, long long* rotations, bool* capped) {
     if (block_jacobi_b(n) == 8)
-        return jacobi_block_sweeps_t<8>(t, n, P, pld, scr, V, ldv, ref_norm, max_sweeps, sc, rotations, capped);
-    return jacobi_block_sweeps_t<4>(t, n, P, pld, scr, V, ldv, ref_norm, max_sweeps, sc, rotations, capped);
+        return jacobi_block_sweeps_t<8>(t, n, P, pld, scr, V, ldv, ref_norm, thr, max_sweeps, sc, rotations, capped);
+    return jacobi_block_sweeps_t<4>(t, n, P, pld, scr, V, ldv, ref_norm, thr, max_sweeps, sc, rotations, capped);
 }
 
 // LieSvdSmall::solve (src/lie_svd_small.rs:296-323) by one team, n <= 64.
@@ -974,8 +1287,16 @@ __device__ inline int jacobi_block_sweeps(const Team& t, int n, double* P, int p
 template <int TS, int G>
 __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm) {
     const int n = job.n;
-    const int np = pad4(n);
-    const int ld = np + 1;
+    const bool mma = team_uses_mma(n, t.nwarps);
+    const int np = team_np(n, mma);
+    const int ld = team_ld(n, mma);
+    // products on the FP64 tensor path or the scalar register tiles
+    auto gemm = [&](auto la, auto lb, auto epi) {
+        if (mma)
+            team_mma(t, np, n, la, lb, epi);
+        else
+            team_gemm<TS>(t, np, n, la, lb, epi);
+    };
     double* X = sm;
     double* T = X + ld * np;
     double* Xn = T + ld * np;
@@ -1029,16 +1350,16 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     bool conv = false, diverged = false;
     int iters = 0;
     for (;;) {
-        team_gemm<TS>(
-            t, np, n, [&](int k, int i) { return X[i * ld + k]; },
+        gemm(
+            [&](int k, int i) { return X[i * ld + k]; },
             [&](int k, int j) { return X[j * ld + k]; },
             [&](int i, int j, double v) { T[j * ld + i] = v; });
         t.sync();
         if (conv || iters == 120) break;  // POLAR_MAX_ITERS, :67
         iters++;
         double d2 = 0.0;
-        team_gemm<TS>(
-            t, np, n, [&](int k, int i) { return X[k * ld + i]; },
+        gemm(
+            [&](int k, int i) { return X[k * ld + i]; },
             [&](int k, int j) { return T[j * ld + k]; },
             [&](int i, int j, double v) {
                 const double x = X[j * ld + i];
@@ -1091,8 +1412,8 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
         load_colmajor(t, job, np, ld, Vb, f, b2);
     }
     t.sync();
-    team_gemm<TS>(
-        t, np, n, [&](int k, int i) { return Q[i * ld + k]; },
+    gemm(
+        [&](int k, int i) { return Q[i * ld + k]; },
         [&](int k, int j) { return Vb[j * ld + k]; },
         [&](int i, int j, double v) { Wb[j * ld + i] = v; });
     t.sync();
@@ -1128,6 +1449,19 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
         pf2 = fma(v, v, pf2);
     }
     const double pref = fmax(sqrt(team_sum(t, pf2, sc->red)), 1e-300);  // syncs Vb
+    // The blocked sweep works on P scaled by a power of two to ||P||_F in
+    // [0.5, 1) (exact; the eigenvalues are scaled back), which keeps its
+    // rotation formula in range.
+    int pe = 0;
+    if (blocked) {
+        frexp(pref, &pe);
+        pe = max(min(pe, 1000), -1000);
+        const double pscale = ldexp(1.0, -pe);
+        for (int idx = t.tid; idx < m * m; idx += t.nthreads) {
+            const int x = idx % m, y = idx / m;
+            Vb[y * pstride + x] *= pscale;
+        }
+    }
     // V = I in the (now free) W buffer; P ping-pongs between Vb and Q's buffer
     double* Vn = Wb;
     for (int idx = t.tid; idx < np * np; idx += t.nthreads) {
@@ -1144,8 +1478,9 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     int par = 0;
     int sweeps;
     if (blocked) {
-        sweeps = jacobi_block_sweeps(t, n, Vb, pstride, Q, Vn, ld, pref, 60 + 20 * n /* :216 */, sc,
-                                     &rotations, &jcap);
+        const double pscale = ldexp(1.0, -pe);
+        sweeps = jacobi_block_sweeps(t, n, Vb, pstride, Q, Vn, ld, pref * pscale, 1e-300 * pscale,
+                                     60 + 20 * n /* :216 */, sc, &rotations, &jcap);
         Pfin = Vb;
         par = 0;
     } else {
@@ -1159,7 +1494,7 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     // ---- eigenvalues on the diagonal, stable descending sort, sigma = max(eig, 0)
     for (int x = t.tid; x < m; x += t.nthreads) {
         const int i = sc->pidx[par][x];
-        if (i < n) sc->sig[i] = Pfin[x * pstride + x];
+        if (i < n) sc->sig[i] = ldexp(Pfin[x * pstride + x], pe);
     }
     t.sync();
     for (int j = t.tid; j < n; j += t.nthreads) {
@@ -1186,15 +1521,14 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     t.sync();
     const int* perm = sc->perm;
     // ---- 4. U = Q V (sorted); orthogonality check (:317-318)
-    team_gemm<TS>(
-        t, np, n, [&](int k, int i) { return Q[k * ld + i]; },
+    gemm(
+        [&](int k, int i) { return Q[k * ld + i]; },
         [&](int k, int j) { return j < n ? Vb[perm[j] * ld + k] : 0.0; },
         [&](int i, int j, double v) { Ub[j * ld + i] = v; });
     t.sync();
     auto orth_of = [&](const double* B) -> double {
         double o2 = 0.0;
-        team_gemm<TS>(
-            t, np, n,
+        gemm(
             [&](int k, int i) { return B[i * ld + k]; },
             [&](int k, int j) { return B[j * ld + k]; },
             [&](int i, int j, double v) {
@@ -1218,8 +1552,8 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
         for (int k = 0; k < n; ++k) smax = fmax(smax, sc->sig[k]);
         const double stol = 1e-12 * fmax(smax, 1.0);
         t.sync();
-        team_gemm<TS>(
-            t, np, n, [&](int k, int i) { return Q[k * ld + i]; },
+        gemm(
+            [&](int k, int i) { return Q[k * ld + i]; },
             [&](int k, int j) { return j < n ? Vb[perm[j] * ld + k] : 0.0; },
             [&](int i, int j, double v) {
                 const double sj = j < n ? sc->sig[perm[j]] : 0.0;
@@ -1253,9 +1587,9 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
         }
         // metrics::compute rel_recon (src/lib.rs:157-159): ||U S V^T - A||_F / ||A||_F
         double r2 = 0.0;
-        team_gemm<TS>(
-            t, np, n, [&](int k, int i) { return Ub[k * ld + i]; },
-            [&](int k, int j) { return j < n ? sc->sig[perm[k]] * Vb[perm[k] * ld + j] : 0.0; },
+        gemm(
+            [&](int k, int i) { return Ub[k * ld + i]; },
+            [&](int k, int j) { return (j < n && k < n) ? sc->sig[perm[k]] * Vb[perm[k] * ld + j] : 0.0; },
             [&](int i, int j, double v) {
                 if (i < n && j < n) {
                     const double d = v - Q[j * ld + i];

@@ -325,7 +325,7 @@ extern "C" lsvd_status lsvd_svd_batched_noalloc_f64(void* stream, int64_t count,
         const int hi = c == 0 ? 4 : (c == 1 ? 8 : c == 2 ? 16 : c == 3 ? 24 : c == 4 ? 32 : c == 5 ? 48 : 64);
         na.cls[c].nwarps = s.nwarps;
         na.cls[c].variant = (s.ts == 4 ? 3 : 0) + (s.g == 16 ? 1 : s.g == 32 ? 2 : 0);
-        na.cls[c].slice = s.nwarps ? team_smem_doubles(hi) : 0;
+        na.cls[c].slice = s.nwarps ? team_smem_doubles(hi, s.nwarps) : 0;
         na.cls[c].pad_ = 0;
         cfga.per_item[c] = s.nwarps == 0 ? kCtaThreads
                                          : (kCtaThreads / (32 * s.nwarps)) * (s.per_team > 0 ? s.per_team : 1);
@@ -360,7 +360,7 @@ extern "C" lsvd_status lsvd_svd_batched_noalloc_f64(void* stream, int64_t count,
     const int grid = ds.num_sms * 2 < count ? ds.num_sms * 2 : int(count);
     noalloc_batched_kernel<<<grid > 0 ? grid : 1, kCtaThreads, smem, st>>>(na);
     const int fgrid = ds.num_sms < count ? ds.num_sms : int(count);
-    noalloc_fallback_kernel<<<fgrid > 0 ? fgrid : 1, kCtaThreads, team_smem_doubles(4) * 8, st>>>(na);
+    noalloc_fallback_kernel<<<fgrid > 0 ? fgrid : 1, kCtaThreads, team_smem_doubles(4, kCtaThreads / 32) * 8, st>>>(na);
     if ((e = cudaGetLastError()) != cudaSuccess) return LSVD_CUDA_ERROR;
     if (flags & LSVD_ASYNC) return LSVD_OK;
     int agg = 0;

@@ -511,7 +511,7 @@ extern "C" lsvd_status lsvd_svd_batched_stream_f64(lsvd_context* ctx, int64_t co
     sa.perm = dPerm;
     sa.want_diag = (flags & LSVD_WANT_DIAG) && dDiag ? 1 : 0;
     sa.agg = agg;
-    const int smem = lsvd::team_smem_doubles(int(n)) * 8;
+    const int smem = lsvd::team_smem_doubles(int(n), lsvd::kCtaThreads / 32) * 8;
     if (n > 32) {
         if ((e = cudaFuncSetAttribute(stream_solve_kernel<4, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem)) != cudaSuccess)
