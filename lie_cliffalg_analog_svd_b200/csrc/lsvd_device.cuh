@@ -787,14 +787,20 @@ __device__ inline int jacobi2pp_sweeps(const Team& t, int n, double* B0, double*
 #define LSVD_BLOCK_JACOBI_MIN_N 33
 #endif
 
-// Block size: 8 from n = 45 (the scratch of n = 40..44 is too small for it), else 4.
-__host__ __device__ constexpr int block_jacobi_b(int n) { return n >= 45 ? 8 : 4; }
-
-__device__ inline int block_jacobi_fits(int n, int scr_doubles) {
-    const int B = block_jacobi_b(n), B2 = 2 * B;
+// Whether the blocked sweep with block size B fits in scr_doubles of scratch:
+// sub-blocks S, R per block pair, then the block-pair table (64 ints).
+__device__ __forceinline__ bool block_jacobi_fits_b(int n, int B, int scr_doubles) {
+    const int B2 = 2 * B;
     const int nbl = (n + B - 1) / B, nbe = nbl + (nbl & 1);
-    // sub-blocks S, R per block pair, then the block-pair table (64 ints)
     return (nbe / 2) * 2 * B2 * (B2 + 2) + 32 <= scr_doubles && nbe >= 2 && (nbe / 2) * B <= 32;
+}
+
+// Block size of the blocked sweep: 8 from n = 41 where the scratch holds it
+// (fewer layers; the team's tensor-path layout does for every n > 32), else
+// 4; 0 when neither fits.
+__device__ __forceinline__ int block_jacobi_b(int n, int scr_doubles) {
+    if (n >= 41 && block_jacobi_fits_b(n, 8, scr_doubles)) return 8;
+    return block_jacobi_fits_b(n, 4, scr_doubles) ? 4 : 0;
 }
 
 // M[:, pair k columns] <- M[:, pair k columns] R_k for every block pair k of
@@ -1270,10 +1276,10 @@ __device__ inline int jacobi_block_sweeps_t(const Team& t, int n, double* P, int
     return sweeps;
 }
 
-__device__ inline int jacobi_block_sweeps(const Team& t, int n, double* P, int pld, double* scr,
+__device__ inline int jacobi_block_sweeps(const Team& t, int n, int bsize, double* P, int pld, double* scr,
                                           double* V, int ldv, double ref_norm, double thr, int max_sweeps,
                                           TeamScratch* sc, long long* rotations, bool* capped) {
-    if (block_jacobi_b(n) == 8)
+    if (bsize == 8)
         return jacobi_block_sweeps_t<8>(t, n, P, pld, scr, V, ldv, ref_norm, thr, max_sweeps, sc, rotations, capped);
     return jacobi_block_sweeps_t<4>(t, n, P, pld, scr, V, ldv, ref_norm, thr, max_sweeps, sc, rotations, capped);
 }
@@ -1425,7 +1431,8 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     // blocked sweep (P in natural order, odd leading dimension m + 1);
     // otherwise the layer-by-layer sweep with P in pair-position order
     // (leading dimension m).
-    const bool blocked = job.rotors == nullptr && n >= LSVD_BLOCK_JACOBI_MIN_N && block_jacobi_fits(n, ld * np);
+    const int bsize = (job.rotors == nullptr && n >= LSVD_BLOCK_JACOBI_MIN_N) ? block_jacobi_b(n, ld * np) : 0;
+    const bool blocked = bsize != 0;
     const int pstride = blocked ? m + 1 : m;
     for (int x = t.tid; x < m; x += t.nthreads) {
         // layer 0: pair k = (m-1, 0) for k = 0, else (k, m-1-k) in ring m-1
@@ -1479,7 +1486,7 @@ __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm)
     int sweeps;
     if (blocked) {
         const double pscale = ldexp(1.0, -pe);
-        sweeps = jacobi_block_sweeps(t, n, Vb, pstride, Q, Vn, ld, pref * pscale, 1e-300 * pscale,
+        sweeps = jacobi_block_sweeps(t, n, bsize, Vb, pstride, Q, Vn, ld, pref * pscale, 1e-300 * pscale,
                                      60 + 20 * n /* :216 */, sc, &rotations, &jcap);
         Pfin = Vb;
         par = 0;
