@@ -1287,8 +1287,9 @@ __device__ inline int jacobi_block_sweeps(const Team& t, int n, int bsize, doubl
 // LieSvdSmall::solve (src/lie_svd_small.rs:296-323) by one team, n <= 64.
 //   1. newton_schulz_polar (:158-183)  X <- 0.5 X (3I - X^T X), FP64 GEMMs in smem
 //   2. P = sym(Q^T A)                  (:305-309)
-//   3. eigensolve of P                 round-robin one-sided Jacobi (numerically
-//      equivalent to the reference's cyclic two-sided sweep on symmetric PSD P)
+//   3. eigensolve of P                 two-sided Jacobi (eigh_jacobi_full, :212-285) in a
+//      parallel order: blocked for n > 32 without a rotor stream, else
+//      layer by layer over round-robin pairs
 //   4. U = Q V, orthogonality check, repair_left_basis_from_right (:185-208, :317-320)
 template <int TS, int G>
 __device__ void small_solve_team(const Team& t, const SmallJob& job, double* sm) {
