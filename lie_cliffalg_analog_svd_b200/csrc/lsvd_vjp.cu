@@ -164,46 +164,58 @@ __global__ void qu_kernel(int m, int n, const double* Q, const double* Ur, doubl
 
 // ------------------------------------------------------------------ adjoint
 
-// C(i, j) = sum_k la(k, i) lb(k, j), 0 <= i < M, 0 <= j < N (both padded to
-// a multiple of TS by the accessors), register tiles of TS x TS per thread
-// interleaved over the block.
-template <int TS, class LA, class LB, class Epi>
-__device__ __forceinline__ void cta_gemm(int M, int N, int K, LA la, LB lb, Epi epi) {
-    const int mt = (M + TS - 1) / TS, nt = (N + TS - 1) / TS;
-    for (int tile = threadIdx.x; tile < mt * nt; tile += blockDim.x) {
-        const int ti = tile % mt, tj = tile / mt;
-        double acc[TS][TS];
+// C(i, j) = sum_k la(k, i) lb(k, j), 0 <= i < M, 0 <= j < N, on the FP64
+// tensor path (mma.sync m8n8k4, lsvd::dmma_8x8x4): the block's warps take
+// blocks of 2 x 4 tiles of 8 x 8 in turn; i >= M, j >= N and k >= K read as
+// zero (no accessor is called there) and only i < M, j < N reach epi.
+template <class LA, class LB, class Epi>
+__device__ __forceinline__ void cta_mma(int M, int N, int K, LA la, LB lb, Epi epi) {
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+    const int mt = (M + 7) >> 3, nt = (N + 7) >> 3;
+    const int mb = (mt + 1) >> 1, nb = (nt + 3) >> 2;
+    for (int blk = warp; blk < mb * nb; blk += nwarps) {
+        const int ti0 = (blk % mb) * 2, tj0 = (blk / mb) * 4;
+        double acc[2][4][2];
 #pragma unroll
-        for (int r = 0; r < TS; ++r)
+        for (int r = 0; r < 2; ++r)
 #pragma unroll
-            for (int c = 0; c < TS; ++c) acc[r][c] = 0.0;
+            for (int c = 0; c < 4; ++c) acc[r][c][0] = acc[r][c][1] = 0.0;
 #pragma unroll 2
-        for (int k = 0; k < K; ++k) {
-            double av[TS], bv[TS];
+        for (int k0 = 0; k0 < K; k0 += 4) {
+            const int k = k0 + q;
+            double av[2], bv[4];
 #pragma unroll
-            for (int r = 0; r < TS; ++r) {
-                const int i = ti + r * mt;
-                av[r] = i < M ? la(k, i) : 0.0;
+            for (int r = 0; r < 2; ++r) {
+                const int i = (ti0 + r) * 8 + g;
+                av[r] = (k < K && i < M) ? la(k, i) : 0.0;
             }
 #pragma unroll
-            for (int c = 0; c < TS; ++c) {
-                const int j = tj + c * nt;
-                bv[c] = j < N ? lb(k, j) : 0.0;
+            for (int c = 0; c < 4; ++c) {
+                const int j = (tj0 + c) * 8 + g;
+                bv[c] = (k < K && j < N) ? lb(k, j) : 0.0;
             }
 #pragma unroll
-            for (int r = 0; r < TS; ++r)
+            for (int r = 0; r < 2; ++r)
 #pragma unroll
-                for (int c = 0; c < TS; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+                for (int c = 0; c < 4; ++c)
+                    if (ti0 + r < mt && tj0 + c < nt) lsvd::dmma_8x8x4(acc[r][c][0], acc[r][c][1], av[r], bv[c]);
         }
 #pragma unroll
-        for (int r = 0; r < TS; ++r)
+        for (int r = 0; r < 2; ++r)
 #pragma unroll
-            for (int c = 0; c < TS; ++c) {
-                const int i = ti + r * mt, j = tj + c * nt;
-                if (i < M && j < N) epi(i, j, acc[r][c]);
-            }
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int i = (ti0 + r) * 8 + g, j = (tj0 + c) * 8 + 2 * q + e;
+                    if (i < M && j < N) epi(i, j, acc[r][c][e]);
+                }
     }
 }
+
+// Leading dimension of the n x n shared buffers: n rounded up to 8, plus 4
+// (= 4 mod 8: the 8 x 4 fragment loads of a half-warp hit 16 distinct banks).
+__host__ __device__ constexpr int vjp_ld(int n) { return ((n + 7) & ~7) + 4; }
 
 struct VjpArgs {
     int m, n;
@@ -225,7 +237,7 @@ struct VjpArgs {
 
 __global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
     extern __shared__ __align__(16) double sh[];
-    const int m = a.m, n = a.n, ld = n + 1;
+    const int m = a.m, n = a.n, ld = vjp_ld(n);
     const size_t mi = blockIdx.x;
     double* V = sh;              // n x ld, row-major
     double* S1 = V + n * ld;
@@ -339,30 +351,30 @@ __global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
     }
     __syncthreads();
     if (Ub)
-        cta_gemm<4>(n, n, m, [&](int k, int i) { return A[size_t(k) * n + i]; },
+        cta_mma(n, n, m, [&](int k, int i) { return A[size_t(k) * n + i]; },
                     [&](int k, int j) { return Ub[size_t(k) * n + j]; },
                     [&](int i, int j, double v) { S1[i * ld + j] = v; });
     __syncthreads();
-    cta_gemm<4>(n, n, n, [&](int k, int i) { return V[k * ld + i]; },
+    cta_mma(n, n, n, [&](int k, int i) { return V[k * ld + i]; },
                 [&](int k, int j) { return S1[k * ld + j]; },
                 [&](int i, int j, double v) { S3[i * ld + j] = si[i] * v; });
     // ---- H = V^T Vbar into S4
     if (Vb)
-        cta_gemm<4>(n, n, n, [&](int k, int i) { return V[k * ld + i]; },
+        cta_mma(n, n, n, [&](int k, int i) { return V[k * ld + i]; },
                     [&](int k, int j) { return Vb[k * n + j]; },
                     [&](int i, int j, double v) { S4[i * ld + j] = v; });
     __syncthreads();
     // ---- M = U^T Qbar V = S^-1 V^T (A^T Qbar) V into S2 (polar cotangent)
     if (Qb) {
-        cta_gemm<4>(n, n, m, [&](int k, int i) { return A[size_t(k) * n + i]; },
+        cta_mma(n, n, m, [&](int k, int i) { return A[size_t(k) * n + i]; },
                     [&](int k, int j) { return Qb[size_t(k) * n + j]; },
                     [&](int i, int j, double v) { S2[i * ld + j] = v; });
         __syncthreads();
-        cta_gemm<4>(n, n, n, [&](int k, int i) { return S2[i * ld + k]; },
+        cta_mma(n, n, n, [&](int k, int i) { return S2[i * ld + k]; },
                     [&](int k, int j) { return V[k * ld + j]; },
                     [&](int i, int j, double v) { S1[i * ld + j] = v; });
         __syncthreads();
-        cta_gemm<4>(n, n, n, [&](int k, int i) { return V[k * ld + i]; },
+        cta_mma(n, n, n, [&](int k, int i) { return V[k * ld + i]; },
                     [&](int k, int j) { return S1[k * ld + j]; },
                     [&](int i, int j, double v) { S2[i * ld + j] = si[i] * v; });
         __syncthreads();
@@ -391,22 +403,22 @@ __global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
     }
     __syncthreads();
     // ---- E = V S^-1 D V^T: S4 = V (S^-1 D), S3 = S4 V^T
-    cta_gemm<4>(n, n, n, [&](int k, int i) { return V[i * ld + k]; },
+    cta_mma(n, n, n, [&](int k, int i) { return V[i * ld + k]; },
                 [&](int k, int j) { return si[k] * S1[k * ld + j]; },
                 [&](int i, int j, double v) { S4[i * ld + j] = v; });
     __syncthreads();
-    cta_gemm<4>(n, n, n, [&](int k, int i) { return S4[i * ld + k]; },
+    cta_mma(n, n, n, [&](int k, int i) { return S4[i * ld + k]; },
                 [&](int k, int j) { return V[j * ld + k]; },
                 [&](int i, int j, double v) { S3[i * ld + j] = v; });
     // ---- Z = V S^-1 V^T into S2 (polar cotangent only)
     if (Qb)
-        cta_gemm<4>(n, n, n, [&](int k, int i) { return V[i * ld + k] * si[k]; },
+        cta_mma(n, n, n, [&](int k, int i) { return V[i * ld + k] * si[k]; },
                     [&](int k, int j) { return V[j * ld + k]; },
                     [&](int i, int j, double v) { S2[i * ld + j] = v; });
     __syncthreads();
     // ---- Abar = A E + Ub S^-1 V^T + Qb Z   (K = n for each term)
     const int K3 = n * (1 + (Ub ? 1 : 0) + (Qb ? 1 : 0));
-    cta_gemm<4>(
+    cta_mma(
         m, n, K3,
         [&](int k, int i) {
             const int part = k / n, kk = k % n;
@@ -423,7 +435,7 @@ __global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
     if (tid == 0) a.status[mi] = 0;
 }
 
-size_t vjp_smem_bytes(int n) { return size_t(5 * n * (n + 1) + 2 * kMaxN) * sizeof(double); }
+size_t vjp_smem_bytes(int n) { return size_t(5 * n * vjp_ld(n) + 2 * kMaxN) * sizeof(double); }
 
 template <class T>
 T* carve(char*& p, size_t count) {
