@@ -48,7 +48,8 @@ using lsvd::kMaxN;
 using lsvd::Team;
 
 constexpr int kVjpThreads = 256;
-constexpr int kChunk = 1024;  // rotations staged in shared memory per replay chunk
+constexpr int kReplayChunk = 512;  // rotations staged in shared memory per replay chunk
+constexpr int kReplayThreads = 64;  // one column of V per thread (n <= 64)
 constexpr int kMaxRows = 4096;
 
 __device__ double block_sum(double v, double* red) {
@@ -229,64 +230,49 @@ struct VjpArgs {
     const double* Sb;  // n, may be null
     const double* Vb;  // n x n (cotangent of V), may be null
     const double* Qb;  // m x n (cotangent of the polar factor U V^T), may be null
-    const double* Vt;  // n x n stored V^T, may be null (then V is replayed)
+    const double* Vt;  // n x n V^T: stored by the forward, or rebuilt by vjp_replay_kernel
+    const int* vstat;  // per matrix replay status (non-zero: stream overflow), may be null
     double gap_tol;
     double* Ab;        // m x n
     int* status;       // per matrix: 0 ok, 1 stream overflow, 2 sigma <= 0
 };
 
-__global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
-    extern __shared__ __align__(16) double sh[];
-    const int m = a.m, n = a.n, ld = vjp_ld(n);
+// V = G_1 (G_2 (... (G_k P))) rebuilt from a matrix's rotor stream, replayed
+// from its end, written as V^T (n x n row-major).  One CTA of kReplayThreads
+// per matrix and a small shared footprint (V plus one chunk of the stream),
+// so that several matrices replay per SM.  A rotation only mixes rows i and
+// j of each column, so the thread that owns column `col` replays the whole
+// stream on it with no barrier; the stream comes through shared memory in
+// chunks with cos/sin computed once.  status: 1 when the count is outside
+// [0, cap] (V^T is then zero).
+__global__ void __launch_bounds__(kReplayThreads) vjp_replay_kernel(int n, const int32_t* perm,
+                                                                   const lsvd_rotor* rotors, int64_t cap,
+                                                                   const int64_t* counts, double* Vt,
+                                                                   int* status) {
+    extern __shared__ __align__(16) double shr[];
+    const int ld = n + 1;  // odd: column walks are bank-conflict free
+    double* V = shr;
+    double2* g_cs = reinterpret_cast<double2*>(V + ((n * ld + 1) & ~1));
+    int* g_ij = reinterpret_cast<int*>(g_cs + kReplayChunk);
+    int* g_safe = g_ij + kReplayChunk;
     const size_t mi = blockIdx.x;
-    double* V = sh;              // n x ld, row-major
-    double* S1 = V + n * ld;
-    double* S2 = S1 + n * ld;
-    double* S3 = S2 + n * ld;
-    double* S4 = S3 + n * ld;
-    double* sg = S4 + n * ld;    // sigma
-    double* si = sg + kMaxN;     // 1/sigma
-    __shared__ int grp_bad;
-    __shared__ double2 g_cs[kChunk];
-    __shared__ int g_ij[kChunk];
-    __shared__ int g_safe[kChunk / 4];
     const int tid = threadIdx.x;
-    const double* A = a.A + mi * size_t(m) * n;
-    const double* Ub = a.Ub ? a.Ub + mi * size_t(m) * n : nullptr;
-    const double* Qb = a.Qb ? a.Qb + mi * size_t(m) * n : nullptr;
-    const double* Vb = a.Vb ? a.Vb + mi * size_t(n) * n : nullptr;
-    const double* Sb = a.Sb ? a.Sb + mi * n : nullptr;
-    double* Ab = a.Ab + mi * size_t(m) * n;
-    const int64_t cnt = a.Vt ? 0 : a.counts[mi];
-    if (tid == 0) grp_bad = 0;
-    __syncthreads();
-    for (int i = tid; i < n; i += blockDim.x) {
-        const double s = a.S[mi * n + i];
-        sg[i] = s;
-        si[i] = s > 0.0 ? 1.0 / s : 0.0;
-        if (!(s > 0.0)) grp_bad = 2;
-    }
-    if (tid == 0 && !a.Vt && (cnt < 0 || cnt > a.cap)) grp_bad = 1;
-    // V <- P, or the stored V (the comparison path that keeps V in memory)
-    const int32_t* perm = a.Vt ? nullptr : a.perm + mi * n;
-    const double* Vst = a.Vt ? a.Vt + mi * size_t(n) * n : nullptr;
-    for (int idx = tid; idx < n * n; idx += blockDim.x) {
-        const int i = idx / n, j = idx % n;
-        V[i * ld + j] = Vst ? Vst[j * n + i] : ((perm[j] == i) ? 1.0 : 0.0);
-    }
-    __syncthreads();
-    if (grp_bad) {
-        for (int idx = tid; idx < m * n; idx += blockDim.x) Ab[idx] = 0.0;
-        if (tid == 0) a.status[mi] = grp_bad;
+    const int64_t cnt = counts[mi];
+    double* vt = Vt + mi * size_t(n) * n;
+    if (cnt < 0 || cnt > cap) {
+        for (int idx = tid; idx < n * n; idx += blockDim.x) vt[idx] = 0.0;
+        if (tid == 0) status[mi] = 1;
         return;
     }
-    // ---- V = G_1 (G_2 (... (G_k P))): the stream replayed from its end.  A
-    // rotation only mixes rows i and j of each column, so the thread that owns
-    // column `col` replays the whole stream on it with no barrier; the stream
-    // comes through shared memory in chunks with cos/sin computed once.
-    const lsvd_rotor* rot = a.rotors + mi * size_t(a.cap);
-    for (int64_t hi = Vst ? 0 : cnt; hi > 0;) {
-        const int64_t lo = hi > kChunk ? hi - kChunk : 0;
+    const int32_t* pm = perm + mi * n;
+    for (int idx = tid; idx < n * n; idx += blockDim.x) {
+        const int i = idx / n, j = idx % n;
+        V[i * ld + j] = (pm[j] == i) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const lsvd_rotor* rot = rotors + mi * size_t(cap);
+    for (int64_t hi = cnt; hi > 0;) {
+        const int64_t lo = hi > kReplayChunk ? hi - kReplayChunk : 0;
         const int len = int(hi - lo);
         for (int e = tid; e < len; e += blockDim.x) {
             const lsvd_rotor r = rot[lo + e];
@@ -300,8 +286,7 @@ __global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
         for (int g = tid; g < len / 4; g += blockDim.x)
             g_safe[g] = rot[lo + 4 * g].round == rot[lo + 4 * g + 3].round;
         __syncthreads();
-        if (tid < n) {
-            const int col = tid;
+        for (int col = tid; col < n; col += blockDim.x) {
             auto one = [&](int e) {
                 const double2 cs = g_cs[e];
                 const int ij = g_ij[e];
@@ -342,6 +327,58 @@ __global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
         }
         __syncthreads();
         hi = lo;
+    }
+    for (int idx = tid; idx < n * n; idx += blockDim.x) {
+        const int j = idx / n, i = idx % n;
+        vt[j * n + i] = V[i * ld + j];
+    }
+    if (tid == 0) status[mi] = 0;
+}
+
+size_t replay_smem_bytes(int n) {
+    return size_t((n * (n + 1) + 1) & ~1) * sizeof(double) + kReplayChunk * (sizeof(double2) + sizeof(int)) +
+           (kReplayChunk / 4) * sizeof(int);
+}
+
+__global__ void __launch_bounds__(kVjpThreads, 1) svd_vjp_kernel(VjpArgs a) {
+    extern __shared__ __align__(16) double sh[];
+    const int m = a.m, n = a.n, ld = vjp_ld(n);
+    const size_t mi = blockIdx.x;
+    double* V = sh;              // n x ld, row-major
+    double* S1 = V + n * ld;
+    double* S2 = S1 + n * ld;
+    double* S3 = S2 + n * ld;
+    double* S4 = S3 + n * ld;
+    double* sg = S4 + n * ld;    // sigma
+    double* si = sg + kMaxN;     // 1/sigma
+    __shared__ int grp_bad;
+    const int tid = threadIdx.x;
+    const double* A = a.A + mi * size_t(m) * n;
+    const double* Ub = a.Ub ? a.Ub + mi * size_t(m) * n : nullptr;
+    const double* Qb = a.Qb ? a.Qb + mi * size_t(m) * n : nullptr;
+    const double* Vb = a.Vb ? a.Vb + mi * size_t(n) * n : nullptr;
+    const double* Sb = a.Sb ? a.Sb + mi * n : nullptr;
+    double* Ab = a.Ab + mi * size_t(m) * n;
+    if (tid == 0) grp_bad = 0;
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) {
+        const double s = a.S[mi * n + i];
+        sg[i] = s;
+        si[i] = s > 0.0 ? 1.0 / s : 0.0;
+        if (!(s > 0.0)) grp_bad = 2;
+    }
+    if (tid == 0 && a.vstat && a.vstat[mi]) grp_bad = a.vstat[mi];
+    // V from V^T (stored by the forward, or rebuilt from the rotor stream)
+    const double* Vst = a.Vt + mi * size_t(n) * n;
+    for (int idx = tid; idx < n * n; idx += blockDim.x) {
+        const int i = idx / n, j = idx % n;
+        V[i * ld + j] = Vst[j * n + i];
+    }
+    __syncthreads();
+    if (grp_bad) {
+        for (int idx = tid; idx < m * n; idx += blockDim.x) Ab[idx] = 0.0;
+        if (tid == 0) a.status[mi] = grp_bad;
+        return;
     }
     // ---- G = U^T Ubar = S^-1 V^T A^T Ubar into S3
     for (int idx = tid; idx < n * ld; idx += blockDim.x) {
@@ -586,7 +623,7 @@ extern "C" lsvd_status lsvd_svd_vjp_f64(lsvd_context* ctx, int64_t count, int64_
     const bool dev = (flags & LSVD_DEVICE_POINTERS) != 0;
     const size_t cnt = size_t(count), mn = size_t(m) * n, nn = size_t(n) * n;
     cudaError_t e;
-    size_t bytes = 8 * 256 + 4 * cnt;
+    size_t bytes = 8 * 256 + 4 * cnt + (Vt ? 0 : nn * 8 * cnt + 4 * cnt + 2 * 256);
     if (!dev)
         bytes += mn * 8 * cnt * (2 + (Ubar ? 1 : 0) + (Qbar ? 1 : 0)) + n * 8 * cnt * (Sbar ? 2 : 1) +
                  ((Vbar ? 1 : 0) + (Vt ? 1 : 0)) * nn * 8 * cnt + 4 * n * cnt + size_t(rotor_cap) * 16 * cnt +
@@ -635,6 +672,22 @@ extern "C" lsvd_status lsvd_svd_vjp_f64(lsvd_context* ctx, int64_t count, int64_
     va.Vt = static_cast<const double*>(pVt);
     va.Ab = dev ? Abar : carve<double>(p, mn * cnt);
     va.status = carve<int>(p, cnt);
+    va.vstat = nullptr;
+    if (!Vt) {
+        // V rebuilt from the rotor streams first, several matrices per SM
+        double* vrep = carve<double>(p, nn * cnt);
+        int* rstat = carve<int>(p, cnt);
+        const size_t rsmem = replay_smem_bytes(int(n));
+        if ((e = cudaFuncSetAttribute(vjp_replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(rsmem))) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "replay smem");
+        vjp_replay_kernel<<<unsigned(cnt), kReplayThreads, rsmem, st>>>(
+            int(n), va.perm, va.rotors, rotor_cap, va.counts, vrep, rstat);
+        ctx->launches++;
+        if ((e = cudaGetLastError()) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "vjp_replay_kernel");
+        va.Vt = vrep;
+        va.vstat = rstat;
+    }
     const size_t smem = vjp_smem_bytes(int(n));
     if ((e = cudaFuncSetAttribute(svd_vjp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) !=
         cudaSuccess)
