@@ -1052,6 +1052,8 @@ __device__ __forceinline__ int inter_rounds(int lane, int lo, int hi, int n, dou
         owner = r + 4 * r1;
     }
     const bool s_writer = B == 8 || lane < 16;
+    bool own_diag = sc[0] == r;
+    if constexpr (NSB == 2) own_diag = own_diag || sc[1] == r;
     const bool p_ok = lo + r < n;
     // round 0 from shared memory
     double app = S[r * SLD + r], aqq = S[(B + r) * SLD + B + r], apq = S[r * SLD + B + r];
@@ -1101,14 +1103,13 @@ __device__ __forceinline__ int inter_rounds(int lane, int lo, int hi, int n, dou
 #pragma unroll
         for (int u = 0; u < NSB; ++u) {
             // rows (p_r, q_r), then columns (p_c, q_c); the diagonal pair-block
-            // takes the exact new diagonal and a zero off-diagonal (:244-249)
+            // is overwritten below with the exact values
             const double y00 = c * xs[u][0] - s * xs[u][2], y10 = s * xs[u][0] + c * xs[u][2];
             const double y01 = c * xs[u][1] - s * xs[u][3], y11 = s * xs[u][1] + c * xs[u][3];
-            const bool dg = sc[u] == r, dr = dg && rot;
-            z[u][0] = dr ? npp : (dg ? xs[u][0] : cc[u] * y00 - ss[u] * y01);
-            z[u][1] = dr ? 0.0 : (dg ? xs[u][1] : ss[u] * y00 + cc[u] * y01);
-            z[u][2] = dr ? 0.0 : (dg ? xs[u][2] : cc[u] * y10 - ss[u] * y11);
-            z[u][3] = dr ? nqq : (dg ? xs[u][3] : ss[u] * y10 + cc[u] * y11);
+            z[u][0] = cc[u] * y00 - ss[u] * y01;
+            z[u][1] = ss[u] * y00 + cc[u] * y01;
+            z[u][2] = cc[u] * y10 - ss[u] * y11;
+            z[u][3] = ss[u] * y10 + cc[u] * y11;
         }
         double zr[NRI][2];
 #pragma unroll
@@ -1124,6 +1125,9 @@ __device__ __forceinline__ int inter_rounds(int lane, int lo, int hi, int n, dou
             zr[v][0] = rcv * xr[v][0] - rsv * xr[v][1];
             zr[v][1] = rsv * xr[v][0] + rcv * xr[v][1];
         }
+        // this round's exact diagonal (the next round's rotation replaces rot, npp, nqq)
+        const bool rot_d = rot;
+        const double npp_d = npp, nqq_d = nqq;
         if (rd + 1 < B) {
             // next round's rotation of pair r, from registers
             double pz = z[0][1];
@@ -1146,6 +1150,15 @@ __device__ __forceinline__ int inter_rounds(int lane, int lo, int hi, int n, dou
                 S[r * SLD + qc[u]] = z[u][1];
                 S[qr * SLD + sc[u]] = z[u][2];
                 S[qr * SLD + qc[u]] = z[u][3];
+            }
+            // the owner of the diagonal pair-block (r, r) of a rotated pair stores the
+            // exact new diagonal and a zero off-diagonal (:244-249) over its values
+            // (without a rotation c = 1, s = 0 left the block unchanged)
+            if (own_diag && rot_d) {
+                S[r * SLD + r] = npp_d;
+                S[r * SLD + qr] = 0.0;
+                S[qr * SLD + r] = 0.0;
+                S[qr * SLD + qr] = nqq_d;
             }
         }
 #pragma unroll
