@@ -113,10 +113,13 @@ LSVD_API int64_t lsvd_context_kernel_launches(const lsvd_context* ctx);
 /* Replaces LieSvdSmall::solve (src/lie_svd_small.rs:296-323): Newton-Schulz
  * polar A = QP, P = sym(Q^T A), Jacobi eigensolve of P, U = QV, left-basis
  * repair.  A n*n (lda), U n*n (ldu), S n (descending), Vt n*n (ldvt).
- * n in 1..64.  `rotors` (may be NULL) receives the accepted rotation stream
- * of the eigensolve, up to rotor_cap entries; *rotor_count gets the number
- * produced.  `perm` (may be NULL, n int32) receives the sort permutation:
- * column k of the returned V is column perm[k] of the rotor-stream product. */
+ * n in 1..64 runs on one CTA with everything in shared memory; `rotors` (may
+ * be NULL) receives the accepted rotation stream of the eigensolve, up to
+ * rotor_cap entries; *rotor_count gets the number produced.  `perm` (may be
+ * NULL, n int32) receives the sort permutation: column k of the returned V is
+ * column perm[k] of the rotor-stream product.  n in 65..16384 runs the
+ * blocked solve of lsvd_svd_large_f64 (rotors, rotor_count and perm must then
+ * be NULL: its block rotations are not a plane-rotation stream). */
 LSVD_API lsvd_status lsvd_small_solve_f64(lsvd_context* ctx, int64_t n, const double* A,
                                           int64_t lda, double* U, int64_t ldu, double* S,
                                           double* Vt, int64_t ldvt, lsvd_diag* diag,
@@ -131,12 +134,50 @@ LSVD_API lsvd_status lsvd_micro_solve_f64(lsvd_context* ctx, int64_t n, const do
 
 /* Replaces LieSvdSmall::solve_rectangular (src/lie_svd_small.rs:340-360):
  * thin SVD of an m*d matrix via QR reduction; k = min(m, d);
- * U m*k, S k, Vt k*d.  min(m, d) in 1..64. */
+ * U m*k, S k, Vt k*d.  min(m, d) in 1..64 on the shared-memory kernels;
+ * larger min(m, d) (up to 16384, max(m, d) up to 65536) through
+ * lsvd_svd_large_f64's thin route. */
 LSVD_API lsvd_status lsvd_small_solve_rectangular_f64(lsvd_context* ctx, int64_t m, int64_t d,
                                                       const double* A, int64_t lda, double* U,
                                                       int64_t ldu, double* S, double* Vt,
                                                       int64_t ldvt, lsvd_diag* diag,
                                                       uint32_t flags);
+
+/* Diagnostics of lsvd_svd_large_f64 (phase times are CUDA-event times on
+ * the context's stream). */
+typedef struct lsvd_large_info {
+    int32_t ns_iters_lowp;   /* TF32/BF16 Newton-Schulz iterations */
+    int32_t ns_iters_fp64;   /* FP64 Newton-Schulz iterations */
+    int32_t sweeps_lowp;     /* low-precision Jacobi sweeps (mixed routes) */
+    int32_t sweeps_fp64;     /* FP64 Jacobi sweeps */
+    int64_t rotations;       /* plane rotations inside the block solves */
+    int32_t flags;           /* LSVD_MAT_* bits */
+    int32_t inner_cap_pairs; /* block pairs whose inner sweeps hit their cap */
+    double last_offdiag;     /* largest |g_i.g_j|/(|g_i||g_j|) seen in the last sweep */
+    double flops_fp64;       /* executed FP64 flops (GEMMs, Gram and apply products) */
+    double flops_lowp;       /* executed TF32/BF16 flops */
+    double ms_polar;         /* Newton-Schulz phase */
+    double ms_eig_lowp;      /* low-precision eigensolve */
+    double ms_eig_fp64;      /* FP64 Jacobi sweeps */
+    double ms_total;         /* device time from the polar phase to U */
+    double rel_recon;        /* with LSVD_WANT_DIAG: ||U S Vt - A||_F / ||A||_F (src/lib.rs:158-159) */
+    double orth_u;           /* ||U^T U - I||_F */
+    double orth_v;           /* ||Vt Vt^T - I||_F */
+} lsvd_large_info;
+
+/* SVD of one large dense matrix (no size class of its own in the reference:
+ * LieSvdSmall::solve, src/lie_svd_small.rs:296-323, and solve_rectangular,
+ * :340-360, run at any size; the reference routes up to n = 512 there,
+ * src/lie_svd_adaptive.rs:71).  A m x n (lda); k = min(m, n); U m x k (ldu),
+ * S k (descending), Vt k x n (ldvt).  FP64: Newton-Schulz polar factor Q of
+ * A (or of A^T when n > m) on the FP64 tensor path, P = sym(Q^T A), V and
+ * sigma = max(lambda, 0) by blocked one-sided Jacobi on P (blocks of 32
+ * columns, 64 x 64 block-pair rotations applied as FP64 tensor products,
+ * convergence flag on the device), U = Q V.  Host or device pointers
+ * (LSVD_DEVICE_POINTERS); synchronous.  `info` may be NULL. */
+LSVD_API lsvd_status lsvd_svd_large_f64(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,
+                                        double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
+                                        lsvd_precision precision, lsvd_large_info* info, uint32_t flags);
 
 /* Batched uneven SVD (no reference counterpart; each matrix takes the route
  * LieSvd::solve's exact tiers take: LieSvdMicro for n<=4
@@ -153,22 +194,25 @@ LSVD_API lsvd_status lsvd_svd_batched_f64(lsvd_context* ctx, int64_t count, cons
                                           uint32_t flags);
 
 /* No counterpart in the reference.  The batched FP64 SVD of
- * lsvd_svd_batched_f64 for callers that cannot allocate device memory: code
- * running while its stream is captured into a CUDA graph (cudaMalloc is not
- * allowed there), latency-critical loops that cannot absorb the device-wide
- * synchronisation of cudaMalloc/cudaFree, and hosts whose device memory
- * belongs to their own allocator or pool.  It allocates nothing: A, U, S, Vt
- * (and diags, may be NULL) are DEVICE buffers of the caller in the packed
- * layout of lsvd_svd_batched_f64, `n` is host memory, `stream` a
- * cudaStream_t of the current device (NULL = legacy default stream), and all
- * working memory is a static device array of LSVD_NOALLOC_SCRATCH_BYTES that
- * every GPU loading the library holds until exit.  At most
- * LSVD_NOALLOC_MAX_COUNT matrices per call (more returns LSVD_UNSUPPORTED).
- * The first call on a device sets that device up (symbol address, kernel
- * attributes): make it before any stream capture.  Calls share the static
- * array, so calls that overlap on a GPU race; serialise them.  With
- * LSVD_ASYNC the call only enqueues work; otherwise it synchronises `stream`
- * and reports the outcome like lsvd_svd_batched_f64. */
+ * lsvd_svd_batched_f64 for callers that cannot allocate device memory:
+ * latency-critical loops that cannot absorb the device-wide synchronisation
+ * of cudaMalloc/cudaFree, and hosts whose device memory belongs to their own
+ * allocator or pool.  It allocates nothing: A, U, S, Vt (and diags, may be
+ * NULL) are DEVICE buffers of the caller in the packed layout of
+ * lsvd_svd_batched_f64, `n` is host memory, `stream` a cudaStream_t of the
+ * current device (NULL = legacy default stream), and all working memory is a
+ * static device array of LSVD_NOALLOC_SCRATCH_BYTES that every GPU loading
+ * the library holds until exit.  At most LSVD_NOALLOC_MAX_COUNT matrices per
+ * call (more returns LSVD_UNSUPPORTED).  The first successful call on a
+ * device sets that device up (the array's device address, kernel
+ * attributes); a failed set-up is retried by the next call.  Calls share the
+ * static array, so calls that overlap on a GPU race; serialise them.
+ * Without LSVD_ASYNC the call synchronises `stream` and reports the outcome
+ * like lsvd_svd_batched_f64.  With LSVD_ASYNC it only enqueues work: `n` is
+ * then copied to the device when the stream reaches the copy, so a pinned
+ * (page-locked) `n` must stay alive and unchanged until the stream has run
+ * past the call (a pageable `n` is read before the call returns); sizes that
+ * left 1..64 in between are caught on the device and nothing is solved. */
 #define LSVD_NOALLOC_MAX_COUNT 65536
 #define LSVD_NOALLOC_SCRATCH_BYTES (4096 + 44 * LSVD_NOALLOC_MAX_COUNT)
 LSVD_API lsvd_status lsvd_svd_batched_noalloc_f64(void* stream, int64_t count, const int32_t* n,
@@ -267,6 +311,16 @@ LSVD_API lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, con
 LSVD_API lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N, int64_t K,
                                        const float* A, const float* B, float* C,
                                        lsvd_precision precision);
+
+/* C = alpha op(A) op(B) + beta C in FP64 (row-major; op(X) = X^T when
+ * trans_x != 0) on the FP64 tensor path (mma.sync m8n8k4): the product
+ * kernel of the FP64 polar iteration and of the large SVD (the reference's
+ * ndarray .dot, src/lie_svd_small.rs:172-173, :305, :313), exposed for
+ * testing.  Device pointers; lda, ldb even and A, B 16-byte aligned;
+ * enqueued on the context's stream without synchronising. */
+LSVD_API lsvd_status lsvd_gemm_f64(lsvd_context* ctx, int32_t trans_a, int32_t trans_b, int64_t M,
+                                   int64_t N, int64_t K, double alpha, const double* A, int64_t lda,
+                                   const double* B, int64_t ldb, double beta, double* C, int64_t ldc);
 
 /* ------------------------------------------- rotor stream and adjoint ---- */
 /* Batched thin SVD of `count` matrices of one shape m x n (m >= n, n <= 64,

@@ -54,6 +54,15 @@ class PolarInfo(C.Structure):
                 ("pad_", C.c_int32)]
 
 
+class LargeInfo(C.Structure):
+    _fields_ = [("ns_iters_lowp", C.c_int32), ("ns_iters_fp64", C.c_int32), ("sweeps_lowp", C.c_int32),
+                ("sweeps_fp64", C.c_int32), ("rotations", C.c_int64), ("flags", C.c_int32),
+                ("inner_cap_pairs", C.c_int32), ("last_offdiag", C.c_double), ("flops_fp64", C.c_double),
+                ("flops_lowp", C.c_double), ("ms_polar", C.c_double), ("ms_eig_lowp", C.c_double),
+                ("ms_eig_fp64", C.c_double), ("ms_total", C.c_double), ("rel_recon", C.c_double),
+                ("orth_u", C.c_double), ("orth_v", C.c_double)]
+
+
 class LsvdError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"lsvd status {status}: {msg}")
@@ -81,6 +90,7 @@ SIGNATURES = {
     "lsvd_small_solve_rectangular_f64": (C.c_int, [P, I64, I64, P, I64, P, I64, P, P, I64, P,
                                                    U32]),
     "lsvd_svd_batched_f64": (C.c_int, [P, I64, P, P, P, P, P, P, C.c_int, U32]),
+    "lsvd_svd_large_f64": (C.c_int, [P, I64, I64, P, I64, P, I64, P, P, I64, C.c_int, P, U32]),
     "lsvd_metrics_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, P, U32]),
     "lsvd_svd_batched_noalloc_f64": (C.c_int, [P, I64, P, P, P, P, P, P, U32]),
     "lsvd_joint_params_for_n": (JointParams, [I64]),
@@ -88,6 +98,8 @@ SIGNATURES = {
     "lsvd_joint_svd_f64": (C.c_int, [P, I64, I64, I64, I64, P, P, P, P, P, P, U32]),
     "lsvd_polar_f64": (C.c_int, [P, I64, I64, P, I64, P, I64, C.c_int, P, U32]),
     "lsvd_gemm_nt_lowp": (C.c_int, [P, I64, I64, I64, P, P, P, C.c_int]),
+    "lsvd_gemm_f64": (C.c_int, [P, C.c_int32, C.c_int32, I64, I64, I64, C.c_double, P, I64, P, I64,
+                                C.c_double, P, I64]),
     "lsvd_svd_batched_stream_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, I64, P, P, P, U32]),
     "lsvd_svd_vjp_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, I64, P, P, P, P, P, P,
                                    C.c_double, P, U32]),

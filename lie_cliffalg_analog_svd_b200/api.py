@@ -85,6 +85,13 @@ def default_context(device: int = 0) -> Context:
     return ctxs[device]
 
 
+PRECISIONS = {"fp64": L.PREC_FP64, "tf32": L.PREC_MIXED_TF32, "bf16": L.PREC_MIXED_BF16}
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
 def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
 
@@ -112,7 +119,8 @@ class LieSvdSmall:
 
     @staticmethod
     def solve(a, ctx: Context | None = None):
-        """Full SVD ``(U, sigma, Vt)`` of a square matrix (n <= 64)."""
+        """Full SVD ``(U, sigma, Vt)`` of a square matrix (n <= 64 on the
+        shared-memory kernels, larger n on the blocked large solve)."""
         r = LieSvdSmall.solve_full(a, ctx=ctx)
         return r.u, r.sigma, r.vt
 
@@ -128,13 +136,16 @@ class LieSvdSmall:
         n = a.shape[0]
         u = np.empty((n, n)); s = np.empty(n); vt = np.empty((n, n))
         d = L.Diag()
-        perm = np.empty(n, dtype=np.int32)
+        small = n <= 64  # the rotor stream and permutation exist on the shared-memory route
+        if rotor_cap and not small:
+            raise L.LsvdError(L.UNSUPPORTED, "LieSvdSmall::solve: rotor stream needs n <= 64")
+        perm = np.empty(n, dtype=np.int32) if small else None
         rot = np.empty(max(rotor_cap, 1), dtype=L.ROTOR_DTYPE) if rotor_cap else None
         cnt = C.c_int64(0)
         st = ctx.lib.lsvd_small_solve_f64(
             ctx.handle, n, _ptr(a), n, _ptr(u), n, _ptr(s), _ptr(vt), n, C.byref(d),
-            _ptr(rot) if rot is not None else None, rotor_cap, C.byref(cnt), _ptr(perm),
-            L.WANT_DIAG if want_diag else 0)
+            _ptr(rot) if rot is not None else None, rotor_cap, C.byref(cnt) if small else None,
+            _ptr(perm) if small else None, L.WANT_DIAG if want_diag else 0)
         if st not in (L.OK, L.NOT_CONVERGED, L.NONFINITE_INPUT, L.ROTOR_OVERFLOW):
             _check(ctx.lib, ctx.handle, st, "LieSvdSmall::solve")
         dd = _diag_dict(d)
@@ -145,7 +156,7 @@ class LieSvdSmall:
 
     @staticmethod
     def solve_rectangular(a, ctx: Context | None = None):
-        """Thin SVD of an m×d matrix (min(m, d) <= 64): U m×k, sigma k, Vt k×d."""
+        """Thin SVD of an m×d matrix: U m×k, sigma k, Vt k×d (k = min(m, d))."""
         ctx = ctx or default_context()
         a = _f64(a)
         if a.ndim != 2 or a.shape[0] == 0 or a.shape[1] == 0:
@@ -158,6 +169,47 @@ class LieSvdSmall:
         if st not in (L.OK, L.NOT_CONVERGED):
             _check(ctx.lib, ctx.handle, st, "LieSvdSmall::solve_rectangular")
         return u, s, vt
+
+
+@dataclass
+class LargeResult:
+    u: object
+    s: object
+    vt: object
+    info: L.LargeInfo
+    diag: dict
+    status: int
+
+
+def svd_large(a, precision: str = "fp64", want_diag: bool = True, ctx: Context | None = None) -> LargeResult:
+    """SVD of one large dense matrix (``lsvd_svd_large_f64``): ``a`` m×n (a
+    numpy array, or a float64 CUDA torch tensor for the device-pointer path);
+    returns the thin U (m×k), S (k), Vt (k×n) with the run's diagnostics."""
+    ctx = ctx or default_context()
+    if _is_torch(a):
+        import torch
+        assert a.is_cuda and a.dtype == torch.float64 and a.is_contiguous()
+        m, n = a.shape
+        k = min(m, n)
+        u = torch.empty((m, k), dtype=torch.float64, device=a.device)
+        s = torch.empty(k, dtype=torch.float64, device=a.device)
+        vt = torch.empty((k, n), dtype=torch.float64, device=a.device)
+        pa, pu, ps, pv = (C.c_void_p(t.data_ptr()) for t in (a, u, s, vt))
+        flags = L.DEVICE_POINTERS
+    else:
+        a = _f64(a)
+        m, n = a.shape
+        k = min(m, n)
+        u = np.empty((m, k)); s = np.empty(k); vt = np.empty((k, n))
+        pa, pu, ps, pv = _ptr(a), _ptr(u), _ptr(s), _ptr(vt)
+        flags = 0
+    info = L.LargeInfo()
+    st = ctx.lib.lsvd_svd_large_f64(ctx.handle, m, n, pa, n, pu, k, ps, pv, n, PRECISIONS[precision],
+                                    C.byref(info), flags | (L.WANT_DIAG if want_diag else 0))
+    if st not in (L.OK, L.NOT_CONVERGED):
+        _check(ctx.lib, ctx.handle, st, "svd_large")
+    diag = {"rel_recon": info.rel_recon, "orth_u": info.orth_u, "orth_v": info.orth_v}
+    return LargeResult(u, s, vt, info, diag, st)
 
 
 class LieSvdMicro:
@@ -225,7 +277,6 @@ class metrics:  # noqa: N801 -- mirrors the Rust module name
                           None if ref is None else out[4])
 
 
-PRECISIONS = {"fp64": L.PREC_FP64, "tf32": L.PREC_MIXED_TF32, "bf16": L.PREC_MIXED_BF16}
 
 
 def packed_offsets(ns) -> tuple[np.ndarray, np.ndarray]:
@@ -249,7 +300,7 @@ def svd_batched(ns, a, precision: str = "fp64", want_diag: bool = False,
     ao, so = packed_offsets(ns)
     prec = PRECISIONS[precision]
     flags = L.WANT_DIAG if want_diag else 0
-    is_torch = type(a).__module__.startswith("torch")
+    is_torch = _is_torch(a)
     if is_torch:
         import torch
         assert a.is_cuda and a.dtype == torch.float64 and a.is_contiguous()
@@ -471,7 +522,7 @@ def polar(a, precision: str = "fp64", ctx: Context | None = None) -> PolarResult
     ctx = ctx or default_context()
     prec = PRECISIONS[precision]
     info = L.PolarInfo()
-    is_torch = type(a).__module__.startswith("torch")
+    is_torch = _is_torch(a)
     if is_torch:
         import torch
         assert a.is_cuda and a.dtype == torch.float64 and a.is_contiguous() and a.dim() == 2
@@ -510,6 +561,31 @@ def gemm_nt_lowp(a, b, precision: str = "tf32", ctx: Context | None = None):
     return c
 
 
+def gemm_f64(a, b, trans_a: bool = False, trans_b: bool = False, alpha: float = 1.0, beta: float = 0.0,
+             c=None, ctx: Context | None = None):
+    """C = alpha op(A) op(B) + beta C in FP64 on the FP64 tensor path (the
+    product kernel of the FP64 polar iteration and the large SVD).  ``a``,
+    ``b`` (and ``c``): float64 CUDA torch tensors, row-major, contiguous rows
+    with an even row stride."""
+    import torch
+    ctx = ctx or default_context()
+    assert a.is_cuda and b.is_cuda and a.dtype == torch.float64 and b.dtype == torch.float64
+    M, K = (a.shape[1], a.shape[0]) if trans_a else a.shape
+    K2, N = (b.shape[1], b.shape[0]) if trans_b else b.shape
+    assert K == K2
+    if c is None:
+        c = torch.zeros((M, N), dtype=torch.float64, device=a.device)
+    assert a.stride(1) == 1 and b.stride(1) == 1 and c.stride(1) == 1
+    # the inputs come from torch's current stream, the product runs on the context's stream
+    torch.cuda.current_stream(a.device).synchronize()
+    st = ctx.lib.lsvd_gemm_f64(ctx.handle, int(trans_a), int(trans_b), M, N, K, alpha,
+                               C.c_void_p(a.data_ptr()), a.stride(0), C.c_void_p(b.data_ptr()), b.stride(0),
+                               beta, C.c_void_p(c.data_ptr()), c.stride(0))
+    _check(ctx.lib, ctx.handle, st, "gemm_f64")
+    ctx.synchronize()
+    return c
+
+
 class SvdStream:
     """Forward of the stream-keeping batched SVD: sigma, sort permutation and
     accepted rotor stream per matrix (U, Vt when requested)."""
@@ -536,10 +612,6 @@ class SvdStream:
         """Bytes of the U and V intermediates this replaces."""
         cnt = self.s.shape[0]
         return cnt * (self.m * self.n + self.n * self.n) * 8
-
-
-def _is_torch(x):
-    return type(x).__module__.startswith("torch")
 
 
 def svd_batched_stream(a, rotor_cap: int | None = None, want_uv: bool = False,

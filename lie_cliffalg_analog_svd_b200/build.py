@@ -63,7 +63,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose or ptxas_verbose, extra), srcs))
-    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcublas"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

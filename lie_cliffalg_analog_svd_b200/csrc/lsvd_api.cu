@@ -26,6 +26,20 @@ lsvd_status lsvd_ctx_fail(lsvd_context* ctx, lsvd_status st, const std::string& 
     return st;
 }
 
+void* lsvd_ctx_pinned(lsvd_context* ctx, size_t bytes) {
+    if (ctx->pinned && ctx->pinned_bytes >= bytes) return ctx->pinned;
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    const size_t sz = std::max(bytes, size_t(4096));
+    if (cudaHostAlloc(&ctx->pinned, sz, cudaHostAllocDefault) != cudaSuccess) {
+        ctx->pinned = nullptr;
+        return nullptr;
+    }
+    ctx->pinned_bytes = sz;
+    return ctx->pinned;
+}
+
 lsvd_status lsvd_ctx_cuda(lsvd_context* ctx, cudaError_t e, const char* where) {
     if (e == cudaSuccess) return LSVD_OK;
     std::string m = std::string(where) + ": " + cudaGetErrorString(e);
@@ -98,9 +112,10 @@ extern "C" lsvd_status lsvd_context_create(int device, lsvd_context** out) {
 lsvd_context::~lsvd_context() {
     cudaSetDevice(device);
     for (auto& kv : plans) kv.second.reset();
-    for (auto* b : {&ws_a, &ws_u, &ws_s, &ws_vt, &ws_diag, &ws_misc, &ws_rot, &ws_polar})
+    for (auto& pp : pipe_plans) pp.reset();
+    for (auto* b : {&ws_a, &ws_u, &ws_s, &ws_vt, &ws_diag, &ws_misc, &ws_rot, &ws_polar, &ws_large})
         b->release();
-    lsvd_destroy_blas(cublas);
+    if (pinned) cudaFreeHost(pinned);
     if (h2d_stream) cudaStreamDestroy(h2d_stream);
     if (d2h_stream) cudaStreamDestroy(d2h_stream);
     if (own_stream && stream) cudaStreamDestroy(stream);
@@ -119,6 +134,8 @@ extern "C" lsvd_status lsvd_context_set_stream(lsvd_context* ctx, void* stream) 
     ctx->stream = static_cast<cudaStream_t>(stream);
     ctx->own_stream = false;
     for (auto& kv : ctx->plans) kv.second->invalidate_graph();
+    for (auto& pp : ctx->pipe_plans)
+        if (pp) pp->invalidate_graph();
     return LSVD_OK;
 }
 
@@ -180,7 +197,7 @@ lsvd_status lsvd_single_small(lsvd_context* ctx, int64_t n, const double* A, int
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (n < 1 || n > kMaxN)
         return lsvd_ctx_fail(ctx, n < 1 ? LSVD_BAD_SHAPE : LSVD_UNSUPPORTED,
-                             "LieSvdSmall::solve: n must be in 1..64");
+                             "LieSvdSmall::solve (shared-memory kernel): n must be in 1..64");
     if (!A || !U || !S || !Vt || lda < n || ldu < n || ldvt < n || rotor_cap < 0 ||
         (rotors && rotor_cap > 0 && !rotor_count))
         return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_small_solve_f64: bad pointer or leading dimension");
@@ -268,6 +285,27 @@ extern "C" lsvd_status lsvd_small_solve_f64(lsvd_context* ctx, int64_t n, const 
                                             double* Vt, int64_t ldvt, lsvd_diag* diag,
                                             lsvd_rotor* rotors, int64_t rotor_cap,
                                             int64_t* rotor_count, int32_t* perm, uint32_t flags) {
+    if (ctx && n > kMaxN) {
+        // beyond the shared-memory kernels: the blocked large solve (no plane-rotation stream)
+        if (rotors || rotor_count || perm)
+            return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "LieSvdSmall::solve: rotor stream and perm need n <= 64");
+        if (!A || !U || !S || !Vt || lda < n || ldu < n || ldvt < n)
+            return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_small_solve_f64: bad pointer or leading dimension");
+        if (n > 16384) return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "LieSvdSmall::solve: n above 16384");
+        cudaSetDevice(ctx->device);
+        lsvd_diag hd;
+        const lsvd_status st = lsvd_large_solve(ctx, n, n, A, lda, U, ldu, S, Vt, ldvt, LSVD_PREC_FP64, nullptr,
+                                                &hd, (flags & LSVD_WANT_DIAG) != 0);
+        if (diag && st != LSVD_CUDA_ERROR && st != LSVD_OUT_OF_MEMORY && st != LSVD_NONFINITE_INPUT) {
+            if (is_dev(flags)) {
+                if (cudaMemcpy(diag, &hd, sizeof(hd), cudaMemcpyHostToDevice) != cudaSuccess)
+                    return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "copy diag out");
+            } else {
+                *diag = hd;
+            }
+        }
+        return st;
+    }
     return lsvd_single_small(ctx, n, A, lda, U, ldu, S, Vt, ldvt, diag, rotors, rotor_cap,
                              rotor_count, perm, flags, 0, false);
 }
@@ -543,12 +581,15 @@ lsvd_status lsvd_run_plan(lsvd_context* ctx, BatchPlan& P, const double* A, doub
     return LSVD_OK;
 }
 
+static bool plan_matches(const BatchPlan& P, int64_t count, const int32_t* n, lsvd_precision prec) {
+    return P.count == count && P.precision == prec && std::equal(P.ns.begin(), P.ns.end(), n);
+}
+
 BatchPlan* lsvd_get_plan(lsvd_context* ctx, int64_t count, const int32_t* n, lsvd_precision prec,
                          lsvd_status* st) {
     const uint64_t key = hash_ns(count, n) ^ (uint64_t(prec) << 61);
     auto it = ctx->plans.find(key);
-    if (it != ctx->plans.end() && it->second->count == count &&
-        std::equal(it->second->ns.begin(), it->second->ns.end(), n)) {
+    if (it != ctx->plans.end() && plan_matches(*it->second, count, n, prec)) {
         *st = LSVD_OK;
         return it->second.get();
     }
@@ -563,9 +604,30 @@ BatchPlan* lsvd_get_plan(lsvd_context* ctx, int64_t count, const int32_t* n, lsv
     return raw;
 }
 
+// The plan of chunk `slot` of the pipelined path: kept in its own slot (not
+// in the shared cache), so two chunks never share staging buffers or a graph.
+static BatchPlan* pipe_plan(lsvd_context* ctx, int slot, int64_t count, const int32_t* n,
+                            lsvd_precision prec, lsvd_status* st) {
+    std::unique_ptr<BatchPlan>& P = ctx->pipe_plans[slot];
+    if (P && plan_matches(*P, count, n, prec)) {
+        *st = LSVD_OK;
+        return P.get();
+    }
+    P = std::make_unique<BatchPlan>();
+    ClassShape shapes[kMaxClasses];
+    lsvd_autotune_shapes(ctx, prec, shapes);
+    *st = build_plan(ctx, count, n, shapes, prec, *P);
+    if (*st != LSVD_OK) {
+        P.reset();
+        return nullptr;
+    }
+    return P.get();
+}
+
 // Host-pointer batches of at least kPipeMin matrices are cut into kPipeChunks
 // contiguous chunks of equal cost (sum of n^3), each with its own plan and
-// staging buffers, so that the copies overlap the solves: H2D of every chunk
+// staging buffers (its own slot, even when two chunks have equal size lists),
+// so that the copies overlap the solves: H2D of every chunk
 // on one copy stream, the solves in order on the context stream, D2H of
 // chunk c on a second copy stream as soon as its solve is done.  The results
 // are those of the unchunked call (every matrix is solved independently).
@@ -603,12 +665,11 @@ static lsvd_status batched_pipelined(lsvd_context* ctx, int64_t count, const int
             soff[c] = s;
         }
     }
-    // every plan stays valid while the chunks run: make room in the cache first
-    if (ctx->plans.size() + C > 16) ctx->plans.clear();
+    static_assert(C <= int(sizeof(ctx->pipe_plans) / sizeof(ctx->pipe_plans[0])), "one slot per chunk");
     BatchPlan* plans[C];
     for (int c = 0; c < C; ++c) {
         lsvd_status st;
-        plans[c] = lsvd_get_plan(ctx, cut[c + 1] - cut[c], n + cut[c], precision, &st);
+        plans[c] = pipe_plan(ctx, c, cut[c + 1] - cut[c], n + cut[c], precision, &st);
         if (!plans[c]) return st;
     }
     cudaEvent_t ev[2 * C + 1];

@@ -86,15 +86,22 @@ struct lsvd_context {
     std::string last_error;
     int64_t launches = 0;
     DeviceBuffer ws_a, ws_u, ws_s, ws_vt, ws_diag, ws_misc, ws_rot, ws_polar;
-    void* cublas = nullptr;  // cublasHandle_t of the large-polar FP64 GEMMs, created on first use
+    DeviceBuffer ws_large;  // large SVD: A, the [G; V] panel store, Gram partials, rotations
     // copy streams of the pipelined host-pointer batched path, created on first use
     cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
     std::unordered_map<uint64_t, std::unique_ptr<BatchPlan>> plans;
+    // one plan per chunk of the pipelined host-pointer path: every chunk owns
+    // its staging buffers, even when two chunks have the same size list
+    std::unique_ptr<BatchPlan> pipe_plans[4];
+    void* pinned = nullptr;  // small page-locked host buffer (device-to-host status reads)
+    size_t pinned_bytes = 0;
     ~lsvd_context();
 };
 
 lsvd_status lsvd_ctx_fail(lsvd_context* ctx, lsvd_status st, const std::string& msg);
 lsvd_status lsvd_ctx_cuda(lsvd_context* ctx, cudaError_t e, const char* where);
+// The context's page-locked host buffer of at least `bytes` (grow-only); NULL on failure.
+void* lsvd_ctx_pinned(lsvd_context* ctx, size_t bytes);
 
 // lsvd_api.cu
 int lsvd_class_of(int n);
@@ -110,7 +117,20 @@ lsvd_status lsvd_single_small(lsvd_context* ctx, int64_t n, const double* A, int
                               int extra_flags, bool host_meta);
 
 // lsvd_polar.cu
-void lsvd_destroy_blas(void* handle);
+// Newton-Schulz polar iteration on the device matrix A (m x n, leading
+// dimension lda) in `precision`, with at most fp64_cap FP64 iterations after
+// the low-precision phase (all iterations for FP64).  The factor is left in
+// the context's polar workspace: *X (m x n, leading dimension *ldx, even).
+lsvd_status lsvd_polar_run(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,
+                           lsvd_precision precision, int fp64_cap, double** X, int64_t* ldx,
+                           lsvd_polar_info* info);
+
+// lsvd_large.cu: SVD of one matrix beyond the shared-memory kernels (rows x
+// cols, either orientation; wide inputs run on the transpose).  U rows x k,
+// S k, Vt k x cols with k = min(rows, cols); pointers host or device.
+lsvd_status lsvd_large_solve(lsvd_context* ctx, int64_t rows, int64_t cols, const double* A, int64_t lda,
+                             double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
+                             lsvd_precision precision, lsvd_large_info* info, lsvd_diag* diag, bool want_diag);
 
 // lsvd_autotune.cu
 void lsvd_autotune_shapes(lsvd_context* ctx, lsvd_precision prec, ClassShape* shapes);

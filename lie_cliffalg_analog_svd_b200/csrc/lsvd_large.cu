@@ -1,0 +1,1270 @@
+// lsvd_large.cu -- SVD of one large dense matrix (n > 64, or thin m x n with
+// n > 64): LieSvdSmall::solve (src/lie_svd_small.rs:296-323) and
+// LieSvdSmall::solve_rectangular (:340-360) beyond the shared-memory-resident
+// batched kernels.
+//
+// FP64 route (the reference's): Newton-Schulz polar A = Q H on the FP64
+// tensor path (lsvd_polar_run), P = sym(Q^T A) (:305-309), the eigenvectors V
+// of P by Jacobi, sigma = max(lambda, 0) in descending order, U = Q V (:313).
+// A tall m x n input runs the polar iteration on the m x n matrix itself
+// (Q^T Q = I), which gives the same thin SVD as the reference's qr_reduce +
+// solve(R) (:340-360); a wide one runs on A^T (:343-348).
+//
+// The eigensolve is eigh_jacobi_full (:212-285) blocked for the GPU: indices
+// are grouped in blocks of 32, and round-robin layers (the circle method of
+// layer_pairs, src/lie_svd_joint.rs:524-539) pair the blocks.  Per sweep the
+// reference's start-of-sweep test off(P) < 1e-13 ||P||_F (offnorm_kernel);
+// per layer
+//   solve2_kernel   diagonalises the 64 x 64 diagonal block of every block
+//                   pair by cyclic Jacobi sweeps (Rutishauser tangent,
+//                   parallel round-robin order) into one orthogonal R
+//   twoside_kernel  P <- R^T P R, one CTA per 64 x 64 block of the
+//                   block-pair triangle (R_a^T P_ab R_b)
+//   apply_kernel    V <- V R on V's column-major store
+// with every product on the FP64 tensor path (mma.sync m8n8k4).  The
+// eigenvalues are the Rayleigh quotients v_j^T P v_j of the converged basis.
+// Parity with the reference is numerical (a parallel order), not bitwise.
+//
+// The one-sided (Hestenes) form of the same blocking -- Gram of a block pair
+// (gram_kernel), its diagonalisation (solve_kernel), and the column update of
+// the panel store H = [G; V] (apply_kernel) -- orthogonalises the columns of
+// an m x n matrix G; the mixed-precision route runs it on G = A V0.
+// Each sweep is one captured CUDA graph; every kernel reads the device-side
+// convergence flag and returns at once after it is set.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "lsvd.h"
+#include "lsvd_dgemm.cuh"
+#include "lsvd_internal.h"
+
+namespace {
+
+using lsvd::dg::cp_async16;
+using lsvd::dg::cp_async_commit;
+using lsvd::dg::cp_async_wait;
+using lsvd::dg::dmma;
+
+constexpr int BW = 32;   // columns per block
+constexpr int PW = 64;   // columns per block pair
+constexpr int GLD = 36;  // gram tile: [64 columns][32 rows + 4], = 4 mod 16
+constexpr int XLD = 68;  // apply tile: [64 columns][64 rows + 4]
+constexpr int MLD = 65;  // 64 x 64 Gram / rotation in the solve kernel
+
+struct SweepState {
+    double scale2;                 // sigma_1^2 estimate of this sweep (largest squared column norm seen)
+    unsigned long long next_scale2;  // bits of the largest squared column norm seen this sweep
+    unsigned long long max_off;  // bits of the largest scaled off-diagonal seen this sweep (>= 0)
+    int rotated;                 // some pair rotated this sweep
+    int converged;
+    int sweeps;                  // completed sweeps
+    int inner_cap;               // pairs whose inner sweeps hit the cap
+    unsigned long long rotations;  // plane rotations applied inside the block solves
+    double last_off;             // max_off of the last completed sweep
+};
+
+// Block pair k of round-robin layer `layer` over nb blocks (nb even).
+__device__ __forceinline__ void block_pair(int nb, int layer, int k, int& a, int& b) {
+    const int ring = nb - 1;
+    if (k == 0) {
+        a = nb - 1;
+        b = layer % ring;
+    } else {
+        a = (layer + k) % ring;
+        b = (layer + ring - k) % ring;
+    }
+}
+
+__device__ __forceinline__ int hrow_of(int col, int P, int Q) {
+    return col < BW ? P * BW + col : Q * BW + (col - BW);
+}
+
+// M partial of block pair blockIdx.x over rows [chunk*kchunk, +kchunk) of G.
+__global__ void __launch_bounds__(256) gram_kernel(const double* __restrict__ H, int64_t ldh, int nb, int layer,
+                                                   int kchunk, int gpad, double* __restrict__ Mpart,
+                                                   const SweepState* __restrict__ stt) {
+    if (stt->converged) return;
+    extern __shared__ __align__(16) double gsmem[];
+    double(*Xs)[PW * GLD] = reinterpret_cast<double(*)[PW * GLD]>(gsmem);  // three stages
+    const int pair = blockIdx.x, chunk = blockIdx.y, nchunk = gridDim.y;
+    int P, Q;
+    block_pair(nb, layer, pair, P, Q);
+    const int k_lo = chunk * kchunk;
+    const int k_hi = min(gpad, k_lo + kchunk);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wi = warp >> 2, wj = warp & 3;
+    const int g = lane >> 2, q = lane & 3;
+    double acc[4][2][2];
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
+    const int KT = k_hi > k_lo ? (k_hi - k_lo) / 32 : 0;
+    auto load = [&](int s, int kt) {
+        const int k0 = k_lo + kt * 32;
+#pragma unroll
+        for (int it = 0; it < 4; ++it) {
+            const int c = tid + it * 256;
+            const int col = c >> 4, kc = (c & 15) * 2;
+            cp_async16(&Xs[s][col * GLD + kc], H + int64_t(hrow_of(col, P, Q)) * ldh + k0 + kc, 16);
+        }
+    };
+    if (KT > 0) load(0, 0);
+    cp_async_commit();
+    if (KT > 1) load(1, 1);
+    cp_async_commit();
+    for (int kt = 0; kt < KT; ++kt) {
+        cp_async_wait<1>();
+        __syncthreads();
+        if (kt + 2 < KT) load((kt + 2) % 3, kt + 2);
+        cp_async_commit();
+        const double* X = Xs[kt % 3];
+#pragma unroll
+        for (int kk = 0; kk < 32; kk += 4) {
+            double a[4], b[2];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) a[t] = X[(wi * 32 + t * 8 + g) * GLD + kk + q];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) b[u] = X[(wj * 16 + u * 8 + g) * GLD + kk + q];
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+#pragma unroll
+                for (int u = 0; u < 2; ++u) dmma(acc[t][u][0], acc[t][u][1], a[t], b[u]);
+        }
+    }
+    cp_async_wait<0>();
+    double* out = Mpart + (int64_t(pair) * nchunk + chunk) * (PW * PW);
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int i = wi * 32 + t * 8 + g, j = wj * 16 + u * 8 + 2 * q;
+            out[i * PW + j] = acc[t][u][0];
+            out[i * PW + j + 1] = acc[t][u][1];
+        }
+}
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) r = fmax(r, red[w]);
+    __syncthreads();
+    return r;
+}
+
+// The scale a Gram entry M_ij is measured against: the larger of
+// sqrt(M_ii M_jj) (the cosine of the two columns) and sqrt(S max(M_ii, M_jj))
+// (the normwise scale, S = sigma_1^2).  A pair is rotated when |M_ij| exceeds
+// tol times this scale: columns far below sigma_1 are orthogonalised down to
+// an absolute error tol sigma_1 |g|, the normwise accuracy of the reference's
+// own stopping rule (off(P) < 1e-13 ||P||_F, src/lie_svd_small.rs:226),
+// instead of to a relative cosine that rounding in the larger columns (about
+// eps sigma_1) puts out of reach.
+__device__ __forceinline__ double pair_scale(double mii, double mjj, double S) {
+    return fmax(sqrt(mii * mjj), sqrt(S * fmax(mii, mjj)));
+}
+
+// Largest scaled off-diagonal |M_ij| / pair_scale over i < j of the 64 x 64
+// Gram in shared memory.
+__device__ __forceinline__ double scaled_offdiag(const double* Ms, double S, double* red) {
+    double off = 0.0;
+    for (int e = threadIdx.x; e < PW * PW; e += 256) {
+        const int i = e >> 6, j = e & 63;
+        if (i < j) {
+            const double d = pair_scale(Ms[i * MLD + i], Ms[j * MLD + j], S);
+            if (d > 0.0) off = fmax(off, fabs(Ms[i * MLD + j]) / d);
+        }
+    }
+    return block_max(off, red);
+}
+
+// Cyclic two-sided Jacobi sweeps (at most inner_max, parallel round-robin
+// order over the 64 indices) on the symmetric 64 x 64 matrix Ms, accumulating
+// the rotations into Rs (which holds I on entry).  rotate(app, aqq, apq)
+// decides whether pair (p, q) is rotated; the sweeps stop after one in which
+// no pair was.  Returns the sweeps run (inner_max + 1 when the cap was hit)
+// and adds the rotations to *cnt.
+template <class Rot>
+__device__ int inner_jacobi(double* Ms, double* Rs, int inner_max, Rot rotate, double* cs, double* sn, int* pa,
+                            int* qa, int* flag, int* cnt) {
+    const int tid = threadIdx.x;
+    int sweep = 0;
+    for (; sweep < inner_max; ++sweep) {
+        if (tid == 0) *flag = 0;
+        __syncthreads();
+        for (int round = 0; round < PW - 1; ++round) {
+            if (tid < 32) {
+                int p, qq;
+                // circle method over 64 indices (src/lie_svd_joint.rs:524-539)
+                if (tid == 0) {
+                    p = PW - 1;
+                    qq = round;
+                } else {
+                    p = (round + tid) % (PW - 1);
+                    qq = (round + PW - 1 - tid) % (PW - 1);
+                }
+                const double app = Ms[p * MLD + p], aqq = Ms[qq * MLD + qq], apq = Ms[p * MLD + qq];
+                double c = 1.0, s = 0.0;
+                if (apq != 0.0 && rotate(app, aqq, apq)) {
+                    // Rutishauser's tangent (src/lie_svd_small.rs:235-242)
+                    const double zeta = (aqq - app) / (2.0 * apq);
+                    const double t = fabs(zeta) > 1e150
+                                         ? 0.5 / zeta
+                                         : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    c = rsqrt(1.0 + t * t);
+                    s = t * c;
+                    atomicAdd(cnt, 1);
+                    *flag = 1;
+                }
+                cs[tid] = c;
+                sn[tid] = s;
+                pa[tid] = p;
+                qa[tid] = qq;
+            }
+            __syncthreads();
+            // M <- J^T M J over 32 x 32 independent 2 x 2 blocks
+            for (int b = tid; b < 32 * 32; b += 256) {
+                const int ka = b >> 5, kb = b & 31;
+                const double ca = cs[ka], sa = sn[ka], cb = cs[kb], sb = sn[kb];
+                if (sa == 0.0 && sb == 0.0) continue;
+                const int ra = pa[ka], rb = qa[ka], ca_ = pa[kb], cb_ = qa[kb];
+                const double x = Ms[ra * MLD + ca_], y = Ms[ra * MLD + cb_];
+                const double z = Ms[rb * MLD + ca_], w = Ms[rb * MLD + cb_];
+                const double x1 = cb * x - sb * y, y1 = sb * x + cb * y;
+                const double z1 = cb * z - sb * w, w1 = sb * z + cb * w;
+                double x2 = ca * x1 - sa * z1, y2 = ca * y1 - sa * w1;
+                double z2 = sa * x1 + ca * z1, w2 = sa * y1 + ca * w1;
+                if (ka == kb) y2 = z2 = 0.0;  // the pair this rotation annihilates
+                Ms[ra * MLD + ca_] = x2;
+                Ms[ra * MLD + cb_] = y2;
+                Ms[rb * MLD + ca_] = z2;
+                Ms[rb * MLD + cb_] = w2;
+            }
+            // R <- R J
+            for (int t = tid; t < PW * 32; t += 256) {
+                const int r = t >> 5, k = t & 31;
+                const double c = cs[k], s = sn[k];
+                if (s == 0.0) continue;
+                const double u = Rs[r * MLD + pa[k]], v = Rs[r * MLD + qa[k]];
+                Rs[r * MLD + pa[k]] = c * u - s * v;
+                Rs[r * MLD + qa[k]] = s * u + c * v;
+            }
+            __syncthreads();
+        }
+        const int any = *flag;
+        __syncthreads();
+        if (!any) break;
+    }
+    return sweep == inner_max ? inner_max + 1 : sweep + 1;
+}
+
+// One-sided route: sums the Gram partials of a block pair, tests it, and
+// diagonalises the Gram into the rotation R (64 x 64, row-major, Rg[pair]).
+// skip[pair] = 1 when the pair needs no rotation.
+__global__ void __launch_bounds__(256) solve_kernel(const double* __restrict__ Mpart, int nchunk,
+                                                    double* __restrict__ Rg, int* __restrict__ skip,
+                                                    SweepState* __restrict__ stt, double tol, int inner_max) {
+    if (stt->converged) return;
+    extern __shared__ __align__(16) double ssmem[];
+    double* Ms = ssmem;             // 64 x 64 Gram, leading dimension 65
+    double* Rs = ssmem + PW * MLD;  // 64 x 64 rotation
+    __shared__ double cs[32], sn[32];
+    __shared__ int pa[32], qa[32];
+    __shared__ double red[8];
+    __shared__ int s_cnt, s_flag;
+    const int pair = blockIdx.x, tid = threadIdx.x;
+    const double* mp = Mpart + int64_t(pair) * nchunk * (PW * PW);
+    for (int e = tid; e < PW * PW; e += 256) {
+        double v = 0.0;
+        for (int c = 0; c < nchunk; ++c) v += mp[int64_t(c) * (PW * PW) + e];
+        Ms[(e >> 6) * MLD + (e & 63)] = v;
+        Rs[(e >> 6) * MLD + (e & 63)] = (e >> 6) == (e & 63) ? 1.0 : 0.0;
+    }
+    if (tid == 0) s_cnt = 0;
+    __syncthreads();
+    const double S = stt->scale2;
+    {
+        double dmax = 0.0;
+        for (int i = tid; i < PW; i += 256) dmax = fmax(dmax, Ms[i * MLD + i]);
+        dmax = block_max(dmax, red);
+        if (tid == 0)
+            atomicMax(&stt->next_scale2, static_cast<unsigned long long>(__double_as_longlong(dmax)));
+    }
+    const double off0 = scaled_offdiag(Ms, S, red);
+    if (tid == 0) atomicMax(&stt->max_off, static_cast<unsigned long long>(__double_as_longlong(off0)));
+    if (!(off0 > tol)) {  // also catches NaN: nothing to rotate
+        if (tid == 0) skip[pair] = 1;
+        return;
+    }
+    const int sw = inner_jacobi(
+        Ms, Rs, inner_max,
+        [&](double app, double aqq, double apq) { return fabs(apq) > tol * pair_scale(app, aqq, S); }, cs, sn,
+        pa, qa, &s_flag, &s_cnt);
+    double* R = Rg + int64_t(pair) * (PW * PW);
+    for (int e = tid; e < PW * PW; e += 256) R[e] = Rs[(e >> 6) * MLD + (e & 63)];
+    if (tid == 0) {
+        skip[pair] = 0;
+        stt->rotated = 1;
+        atomicAdd(&stt->rotations, (unsigned long long)s_cnt);
+        if (sw > inner_max) atomicAdd(&stt->inner_cap, 1);
+    }
+}
+
+// Index of column/row `c` (0..63) of block pair (P, Q) in the full matrix.
+__device__ __forceinline__ int pair_index(int c, int P, int Q) { return hrow_of(c, P, Q); }
+
+// Two-sided route, sweep start: off(P)^2 = sum_{p<q} P_pq^2 over the
+// symmetric P (npad x npad, row-major); the solve stops before the sweep when
+// sqrt(off) < tol_ref ||P0||_F -- the test eigh_jacobi_full makes at the start
+// of every sweep (src/lie_svd_small.rs:220-228).  One CTA.
+__global__ void __launch_bounds__(1024) offnorm_kernel(const double* __restrict__ P, int64_t ldp, int n,
+                                                       SweepState* __restrict__ stt, double limit) {
+    if (stt->converged) return;
+    __shared__ double red[32];
+    double s = 0.0;
+    const int64_t tot = int64_t(n) * n;
+    for (int64_t e = threadIdx.x; e < tot; e += 1024) {
+        const int64_t i = e / n, j = e % n;
+        if (i < j) {
+            const double v = P[i * ldp + j];
+            s += v * v;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 32; ++w) t += red[w];
+        const double off = sqrt(t);
+        stt->last_off = off;
+        if (off < limit) stt->converged = 1;
+    }
+}
+
+// Two-sided route: gathers the 64 x 64 diagonal block of block pair
+// blockIdx.x from P, diagonalises it (rotations of |a_pq| > tau, the
+// reference rotating every |a_pq| >= 1e-300, src/lie_svd_small.rs:233-235),
+// and writes R / skip like solve_kernel.
+__global__ void __launch_bounds__(256) solve2_kernel(const double* __restrict__ P, int64_t ldp, int nb, int layer,
+                                                     double* __restrict__ Rg, int* __restrict__ skip,
+                                                     SweepState* __restrict__ stt, double tau, int inner_max) {
+    if (stt->converged) return;
+    extern __shared__ __align__(16) double ssmem[];
+    double* Ms = ssmem;
+    double* Rs = ssmem + PW * MLD;
+    __shared__ double cs[32], sn[32];
+    __shared__ int pa[32], qa[32];
+    __shared__ double red[8];
+    __shared__ int s_cnt, s_flag;
+    const int pair = blockIdx.x, tid = threadIdx.x;
+    int Pb, Qb;
+    block_pair(nb, layer, pair, Pb, Qb);
+    for (int e = tid; e < PW * PW; e += 256) {
+        const int i = e >> 6, j = e & 63;
+        Ms[i * MLD + j] = P[int64_t(pair_index(i, Pb, Qb)) * ldp + pair_index(j, Pb, Qb)];
+        Rs[i * MLD + j] = i == j ? 1.0 : 0.0;
+    }
+    if (tid == 0) s_cnt = 0;
+    __syncthreads();
+    double off = 0.0;
+    for (int e = tid; e < PW * PW; e += 256) {
+        const int i = e >> 6, j = e & 63;
+        if (i < j) off = fmax(off, fabs(Ms[i * MLD + j]));
+    }
+    off = block_max(off, red);
+    if (!(off > tau)) {
+        if (tid == 0) skip[pair] = 1;
+        return;
+    }
+    const int sw = inner_jacobi(
+        Ms, Rs, inner_max, [&](double, double, double apq) { return fabs(apq) > tau; }, cs, sn, pa, qa, &s_flag,
+        &s_cnt);
+    double* R = Rg + int64_t(pair) * (PW * PW);
+    for (int e = tid; e < PW * PW; e += 256) R[e] = Rs[(e >> 6) * MLD + (e & 63)];
+    if (tid == 0) {
+        skip[pair] = 0;
+        stt->rotated = 1;
+        atomicAdd(&stt->rotations, (unsigned long long)s_cnt);
+        if (sw > inner_max) atomicAdd(&stt->inner_cap, 1);
+    }
+}
+
+// Two-sided route: P <- R^T P R for the block-diagonal R of one layer.  CTA
+// (a, b), a <= b, computes the 64 x 64 block C = R_a^T P_ab R_b of block
+// pairs a and b (R = I for a skipped pair) and writes C to P_ab and C^T to
+// P_ba; the blocks are disjoint, so every block of P is written once.
+// Both products on the FP64 tensor path.
+__global__ void __launch_bounds__(256, 2) twoside_kernel(double* __restrict__ P, int64_t ldp, int nb, int layer,
+                                                         const double* __restrict__ Rg,
+                                                         const int* __restrict__ skip,
+                                                         const SweepState* __restrict__ stt) {
+    if (stt->converged) return;
+    // (a, b) from the linear CTA index over the upper triangle of npairs x npairs
+    const int npairs = nb / 2;
+    int a = 0, rem = blockIdx.x;
+    while (rem >= npairs - a) {
+        rem -= npairs - a;
+        ++a;
+    }
+    const int b = a + rem;
+    const bool ra = !skip[a], rb = !skip[b];
+    if (!ra && !rb) return;
+    extern __shared__ __align__(16) double tsm[];
+    double* Ps = tsm;                // P_ab, then T = P_ab R_b   [64][68]
+    double* Ra = tsm + PW * XLD;     // R_a                        [64][68]
+    double* Rb = tsm + 2 * PW * XLD; // R_b                        [64][68]
+    int Pa, Qa, Pb2, Qb2;
+    block_pair(nb, layer, a, Pa, Qa);
+    block_pair(nb, layer, b, Pb2, Qb2);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wi = warp >> 1, wj = warp & 1;  // 4 x 2 warps; warp tile 16 rows x 32 columns
+    const int g = lane >> 2, q = lane & 3;
+    for (int c = tid; c < PW * PW / 2; c += 256) {
+        const int i = c >> 5, jc = (c & 31) * 2;
+        cp_async16(&Ps[i * XLD + jc], P + int64_t(pair_index(i, Pa, Qa)) * ldp + pair_index(jc, Pb2, Qb2), 16);
+        if (ra) cp_async16(&Ra[i * XLD + jc], Rg + int64_t(a) * (PW * PW) + i * PW + jc, 16);
+        if (rb) cp_async16(&Rb[i * XLD + jc], Rg + int64_t(b) * (PW * PW) + i * PW + jc, 16);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    double acc[2][4][2];
+    if (rb) {  // T = P_ab R_b
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
+#pragma unroll 4
+        for (int k0 = 0; k0 < PW; k0 += 4) {
+            double av[2], bv[4];
+#pragma unroll
+            for (int t = 0; t < 2; ++t) av[t] = Ps[(wi * 16 + t * 8 + g) * XLD + k0 + q];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) bv[u] = Rb[(k0 + q) * XLD + wj * 32 + u * 8 + g];
+#pragma unroll
+            for (int t = 0; t < 2; ++t)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) dmma(acc[t][u][0], acc[t][u][1], av[t], bv[u]);
+        }
+        __syncthreads();  // every warp has read P_ab
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int i = wi * 16 + t * 8 + g, j = wj * 32 + u * 8 + 2 * q;
+                Ps[i * XLD + j] = acc[t][u][0];
+                Ps[i * XLD + j + 1] = acc[t][u][1];
+            }
+        __syncthreads();
+    }
+    // C = R_a^T T (or C = T when a is skipped)
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
+    if (ra) {
+#pragma unroll 4
+        for (int k0 = 0; k0 < PW; k0 += 4) {
+            double av[2], bv[4];
+#pragma unroll
+            for (int t = 0; t < 2; ++t) av[t] = Ra[(k0 + q) * XLD + wi * 16 + t * 8 + g];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) bv[u] = Ps[(k0 + q) * XLD + wj * 32 + u * 8 + g];
+#pragma unroll
+            for (int t = 0; t < 2; ++t)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) dmma(acc[t][u][0], acc[t][u][1], av[t], bv[u]);
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int i = wi * 16 + t * 8 + g, j = wj * 32 + u * 8 + 2 * q;
+                acc[t][u][0] = Ps[i * XLD + j];
+                acc[t][u][1] = Ps[i * XLD + j + 1];
+            }
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const int i = wi * 16 + t * 8 + g;
+        const int gi = pair_index(i, Pa, Qa);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = wj * 32 + u * 8 + 2 * q;
+            const int gj = pair_index(j, Pb2, Qb2);  // j, j + 1 in the same 32-block
+            *reinterpret_cast<double2*>(P + int64_t(gi) * ldp + gj) = make_double2(acc[t][u][0], acc[t][u][1]);
+            if (a != b) {
+                P[int64_t(gj) * ldp + gi] = acc[t][u][0];
+                P[int64_t(gj + 1) * ldp + gi] = acc[t][u][1];
+            }
+        }
+    }
+}
+
+// [G_p G_q; V_p V_q] <- [G_p G_q; V_p V_q] R over rows [chunk*rows, +rows) of H.
+// Computed transposed, C'(j, row) = sum_i R(i, j) H(row, col_i), so that the
+// result lands on H's column-major storage in 16-byte pairs.
+__global__ void __launch_bounds__(256, 2) apply_kernel(double* __restrict__ H, int64_t ldh, int nb, int layer,
+                                                       int rows, const double* __restrict__ Rg,
+                                                       const int* __restrict__ skip,
+                                                       const SweepState* __restrict__ stt) {
+    if (stt->converged) return;
+    const int pair = blockIdx.x;
+    if (skip[pair]) return;
+    extern __shared__ __align__(16) double asmem[];
+    double* Rs = asmem;                 // [64][68]
+    double* Xs0 = asmem + PW * XLD;     // two [64][68] stages
+    int P, Q;
+    block_pair(nb, layer, pair, P, Q);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wj = warp >> 1, wr = warp & 1;  // 4 (j) x 2 (rows); warp tile 16 j x 32 rows
+    const int g = lane >> 2, q = lane & 3;
+    const double* R = Rg + int64_t(pair) * (PW * PW);
+    for (int c = tid; c < PW * PW / 2; c += 256) {
+        const int i = c >> 5, jc = (c & 31) * 2;
+        cp_async16(&Rs[i * XLD + jc], R + i * PW + jc, 16);
+    }
+    cp_async_commit();
+    const int64_t r_lo = int64_t(blockIdx.y) * rows;
+    const int64_t r_hi = min(int64_t(ldh), r_lo + rows);
+    const int NT = r_hi > r_lo ? int((r_hi - r_lo) / 64) : 0;
+    auto load = [&](int s, int t) {
+        double* X = Xs0 + s * PW * XLD;
+        const int64_t r0 = r_lo + int64_t(t) * 64;
+#pragma unroll
+        for (int it = 0; it < 8; ++it) {
+            const int c = tid + it * 256;
+            const int i = c >> 5, rc = (c & 31) * 2;
+            cp_async16(&X[i * XLD + rc], H + int64_t(hrow_of(i, P, Q)) * ldh + r0 + rc, 16);
+        }
+    };
+    if (NT > 0) load(0, 0);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    // A = R^T fragments for this warp's 16 columns j over all 64 i, kept in registers
+    double ra[16][2];
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk)
+#pragma unroll
+        for (int t = 0; t < 2; ++t) ra[kk][t] = Rs[(kk * 4 + q) * XLD + wj * 16 + t * 8 + g];
+    for (int t = 0; t < NT; ++t) {
+        if (t + 1 < NT) load((t + 1) & 1, t + 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const double* X = Xs0 + (t & 1) * PW * XLD;
+        double acc[2][4][2];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[a][u][0] = acc[a][u][1] = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            double b[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) b[u] = X[(kk * 4 + q) * XLD + wr * 32 + u * 8 + g];
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) dmma(acc[a][u][0], acc[a][u][1], ra[kk][a], b[u]);
+        }
+        const int64_t r0 = r_lo + int64_t(t) * 64;
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            const int j = wj * 16 + a * 8 + g;
+            double* hcol = H + int64_t(hrow_of(j, P, Q)) * ldh + r0 + wr * 32 + 2 * q;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                *reinterpret_cast<double2*>(hcol + u * 8) = make_double2(acc[a][u][0], acc[a][u][1]);
+        }
+        __syncthreads();  // the stage just read is the next prefetch's target
+    }
+    cp_async_wait<0>();
+}
+
+// End of a sweep: converged when no pair rotated, or when every pair started
+// the sweep within tol_conv -- the sweep's own rotations then leave every
+// scaled off-diagonal at about tol_conv^2 (Jacobi's quadratic convergence),
+// far below the rotation threshold.
+__global__ void sweep_end_kernel(SweepState* stt, double tol_conv) {
+    if (stt->converged) return;
+    stt->sweeps += 1;
+    const double off = __longlong_as_double(static_cast<long long>(stt->max_off));
+    stt->last_off = off;
+    if (!stt->rotated || off <= tol_conv) stt->converged = 1;
+    stt->rotated = 0;
+    stt->max_off = 0ull;
+    stt->scale2 = fmax(stt->scale2, __longlong_as_double(static_cast<long long>(stt->next_scale2)));
+    stt->next_scale2 = 0ull;
+}
+
+// H (column j = [g_j (gpad rows); v_j (npad rows)]) from the symmetric part of
+// P (n x n, ld) scaled by `scale`; V = I; padding zero.
+__global__ void fill_h_sym_kernel(const double* P, int64_t ld, int n, double scale, double* H, int64_t ldh,
+                                  int gpad, int npad) {
+    const int64_t tot = int64_t(npad) * ldh;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * blockDim.x) {
+        const int j = int(e / ldh), r = int(e % ldh);
+        double v = 0.0;
+        if (r < gpad) {
+            if (j < n && r < n) v = 0.5 * scale * (P[int64_t(r) * ld + j] + P[int64_t(j) * ld + r]);
+        } else {
+            v = (r - gpad) == j ? 1.0 : 0.0;
+        }
+        H[e] = v;
+    }
+}
+
+// P2 (npad x npad) = scale sym(P) with zero padding; Vc (npad x npad) = I.
+__global__ void fill_p2v_kernel(const double* P, int64_t ld, int n, double scale, double* P2, double* Vc, int npad) {
+    const int64_t tot = int64_t(npad) * npad;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * blockDim.x) {
+        const int r = int(e / npad), j = int(e % npad);
+        P2[e] = (r < n && j < n) ? 0.5 * scale * (P[int64_t(r) * ld + j] + P[int64_t(j) * ld + r]) : 0.0;
+        Vc[e] = r == j ? 1.0 : 0.0;
+    }
+}
+
+// sigma_j = ||g_j||, and the sign test of the plain route: lambda_j = v_j . g_j
+// (G = P V, so g_j = lambda_j v_j at convergence).  One warp per column.
+__global__ void colnorm_kernel(const double* H, int64_t ldh, int n, int gm, int gpad, int sign_test, double* sig) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const double* col = H + int64_t(warp) * ldh;
+    double s2 = 0.0, dot = 0.0;
+    for (int r = lane; r < gm; r += 32) {
+        const double gv = col[r];
+        s2 += gv * gv;
+        if (sign_test) dot += gv * col[gpad + r];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        dot += __shfl_xor_sync(0xffffffffu, dot, o);
+    }
+    if (lane == 0) sig[warp] = (sign_test && !(dot > 0.0)) ? 0.0 : sqrt(s2);
+}
+
+// lambda_j = v_j . (P0 v_j): the Rayleigh quotients of the original P0 for
+// the converged basis (Vc row j = v_j, Gt row j = (P0 v_j)^T).  One warp per j.
+__global__ void rayleigh_kernel(const double* Vc, int64_t ldv, const double* Gt, int64_t ldg, int n, double* lam) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s += Vc[int64_t(warp) * ldv + i] * Gt[int64_t(warp) * ldg + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) lam[warp] = s;
+}
+
+// Vt (n x n, ldv): row k = v_{perm[k]} (H's V part).
+__global__ void gather_vt_kernel(const double* H, int64_t ldh, int gpad, int n, const int* perm, double* Vt,
+                                 int64_t ldv) {
+    const int64_t tot = int64_t(n) * n;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * blockDim.x) {
+        const int k = int(e / n), i = int(e % n);
+        Vt[int64_t(k) * ldv + i] = H[int64_t(perm[k]) * ldh + gpad + i];
+    }
+}
+
+__global__ void frob2_part_kernel(int m, int n, const double* A, int64_t lda, double* part) {
+    __shared__ double red[256];
+    double s = 0.0;
+    const int64_t tot = int64_t(m) * n;
+    for (int64_t e = blockIdx.x * int64_t(256) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * 256) {
+        const double v = A[(e / n) * lda + e % n];
+        s += v * v;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// Sum of squares of (X - I) over an n x n matrix (ld), or of X - Y over m x n
+// (Y != nullptr, ldy), per block.
+__global__ void diff2_kernel(int m, int n, const double* X, int64_t ldx, const double* Y, int64_t ldy,
+                             double* part) {
+    __shared__ double red[256];
+    double s = 0.0;
+    const int64_t tot = int64_t(m) * n;
+    for (int64_t e = blockIdx.x * int64_t(256) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * 256) {
+        const int64_t i = e / n, j = e % n;
+        const double d = X[i * ldx + j] - (Y ? Y[i * ldy + j] : (i == j ? 1.0 : 0.0));
+        s += d * d;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// X (m x n, ldx) columns scaled by s (U diag(S)).
+__global__ void scale_cols_kernel(int m, int n, const double* X, int64_t ldx, const double* s, double* Y,
+                                  int64_t ldy) {
+    const int64_t tot = int64_t(m) * n;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = e / n, j = e % n;
+        Y[i * ldy + j] = X[i * ldx + j] * s[j];
+    }
+}
+
+__global__ void sum_parts_kernel(int count, const double* part, double* out) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < count; i += 256) s += part[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+// out (cols x rows, ldo) = in (rows x cols, ldi)^T through 32 x 32 shared tiles.
+__global__ void transpose_kernel(int rows, int cols, const double* in, int64_t ldi, double* out, int64_t ldo) {
+    __shared__ double tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    for (int r0 = blockIdx.y * 32; r0 < rows; r0 += gridDim.y * 32)
+        for (int c0 = blockIdx.x * 32; c0 < cols; c0 += gridDim.x * 32) {
+            for (int k = ty; k < 32; k += 8) {
+                const int r = r0 + k, c = c0 + tx;
+                tile[k][tx] = (r < rows && c < cols) ? in[int64_t(r) * ldi + c] : 0.0;
+            }
+            __syncthreads();
+            for (int k = ty; k < 32; k += 8) {
+                const int c = c0 + k, r = r0 + tx;
+                if (c < cols && r < rows) out[int64_t(c) * ldo + r] = tile[tx][k];
+            }
+            __syncthreads();
+        }
+}
+
+constexpr int kApplySmem = 3 * PW * XLD * 8;  // R + two stages: 104448 bytes
+constexpr int kGramSmem = 3 * PW * GLD * 8;   // three stages: 55296 bytes
+constexpr int kSolveSmem = 2 * PW * MLD * 8;  // M and R: 66560 bytes
+constexpr int kTwoSmem = 3 * PW * XLD * 8;    // P_ab / T, R_a, R_b: 104448 bytes
+
+struct EventTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    EventTimer() {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~EventTimer() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    void start(cudaStream_t s) { cudaEventRecord(a, s); }
+    void stop(cudaStream_t s) { cudaEventRecord(b, s); }
+    double ms() {
+        float t = 0.f;
+        return cudaEventElapsedTime(&t, a, b) == cudaSuccess ? double(t) : 0.0;
+    }
+};
+
+}  // namespace
+
+// Blocked one-sided Jacobi on H = [G; V] (see the file comment).  H: npad
+// columns of ldh doubles (G rows [0, gm), zero rows up to gpad, V rows
+// [gpad, gpad + npad)).  Returns the completed sweeps, rotations and the last
+// sweep's largest relative off-diagonal through the out-parameters.
+static lsvd_status run_sweeps(lsvd_context* ctx, double* H, int64_t ldh, int gm, int gpad, int npad, double tol,
+                              double tol_conv, double scale2, int max_sweeps, int inner_max, char* ws,
+                              int* sweeps_out, int64_t* rot_out, double* off_out, int* inner_cap_out,
+                              double* ms_out) {
+    cudaStream_t st = ctx->stream;
+    const int nb = npad / BW;
+    const int npairs = nb / 2;
+    const int sms = ctx->num_sms;
+    int nchunk = std::max(1, std::min(gpad / 64, (3 * sms + npairs - 1) / npairs));
+    int kchunk = ((gpad / 64 + nchunk - 1) / nchunk) * 64;
+    nchunk = (gpad + kchunk - 1) / kchunk;
+    int napply = std::max(1, (4 * sms + npairs - 1) / npairs);
+    int rows = int(((ldh / 64 + napply - 1) / napply) * 64);
+    napply = int((ldh + rows - 1) / rows);
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    char* p = ws;
+    SweepState* stt = reinterpret_cast<SweepState*>(p); p += al(sizeof(SweepState));
+    int* skip = reinterpret_cast<int*>(p); p += al(size_t(npairs) * 4);
+    double* Rg = reinterpret_cast<double*>(p); p += al(size_t(npairs) * PW * PW * 8);
+    double* Mpart = reinterpret_cast<double*>(p);
+    SweepState init;
+    std::memset(&init, 0, sizeof(init));
+    init.scale2 = scale2;
+    SweepState* hinit = static_cast<SweepState*>(lsvd_ctx_pinned(ctx, 2 * sizeof(SweepState)));
+    if (!hinit) return lsvd_ctx_fail(ctx, LSVD_OUT_OF_MEMORY, "large: pinned state");
+    *hinit = init;
+    cudaError_t e = cudaMemcpyAsync(stt, hinit, sizeof(SweepState), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // hinit is reused for the sweep reads below
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGramSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem);
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: sweep setup");
+    // one sweep = nb - 1 layers of (gram, solve, apply) + the sweep-end test, captured once
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: begin capture");
+    for (int layer = 0; layer < nb - 1; ++layer) {
+        gram_kernel<<<dim3(npairs, nchunk), 256, kGramSmem, st>>>(H, ldh, nb, layer, kchunk, gpad, Mpart, stt);
+        solve_kernel<<<npairs, 256, kSolveSmem, st>>>(Mpart, nchunk, Rg, skip, stt, tol, inner_max);
+        apply_kernel<<<dim3(npairs, napply), 256, kApplySmem, st>>>(H, ldh, nb, layer, rows, Rg, skip, stt);
+    }
+    sweep_end_kernel<<<1, 1, 0, st>>>(stt, tol_conv);
+    cudaError_t e2 = cudaGetLastError();
+    e = cudaStreamEndCapture(st, &graph);
+    if (e2 != cudaSuccess || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return lsvd_ctx_cuda(ctx, e2 != cudaSuccess ? e2 : e, "large: sweep capture");
+    }
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: graph instantiate");
+    const int launches_per_sweep = 3 * (nb - 1) + 1;
+    // The host runs one sweep ahead of the flag it reads: sweep k+1 is queued
+    // before sweep k's state (copied into pinned memory after sweep k) is
+    // examined; once the flag is set, a queued sweep's kernels return at once.
+    SweepState* hst = static_cast<SweepState*>(lsvd_ctx_pinned(ctx, 2 * sizeof(SweepState)));
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    lsvd_status out = LSVD_OK;
+    if (!hst) out = lsvd_ctx_fail(ctx, LSVD_OUT_OF_MEMORY, "large: pinned state");
+    for (int i = 0; i < 2 && out == LSVD_OK; ++i)
+        if ((e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming)) != cudaSuccess)
+            out = lsvd_ctx_cuda(ctx, e, "large: events");
+    EventTimer tm;
+    tm.start(st);
+    int launched = 0;
+    while (out == LSVD_OK && launched < max_sweeps) {
+        const int k = launched;
+        if ((e = cudaGraphLaunch(exec, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(&hst[k & 1], stt, sizeof(SweepState), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaEventRecord(ev[k & 1], st)) != cudaSuccess) {
+            out = lsvd_ctx_cuda(ctx, e, "large: sweep launch");
+            break;
+        }
+        ++launched;
+        ctx->launches += launches_per_sweep;
+        if (k >= 1) {
+            if ((e = cudaEventSynchronize(ev[(k - 1) & 1])) != cudaSuccess) {
+                out = lsvd_ctx_cuda(ctx, e, "large: sweep sync");
+                break;
+            }
+            if (hst[(k - 1) & 1].converged) break;
+        }
+    }
+    tm.stop(st);
+    SweepState hs;
+    std::memset(&hs, 0, sizeof(hs));
+    if (out == LSVD_OK) {
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+            out = lsvd_ctx_cuda(ctx, e, "large: sweep state");
+        else
+            hs = hst[(launched - 1) & 1];
+    }
+    for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+    cudaGraphExecDestroy(exec);
+    if (out != LSVD_OK) return out;
+    *sweeps_out = hs.sweeps;
+    *rot_out = hs.rotations;
+    *off_out = hs.last_off;
+    *inner_cap_out = hs.inner_cap;
+    *ms_out = tm.ms();
+    return hs.converged ? LSVD_OK : LSVD_NOT_CONVERGED;
+}
+
+// Blocked two-sided Jacobi on the symmetric P (npad x npad, row-major, padding
+// zero) accumulating V into Vc (row j = v_j; I on entry): per sweep the
+// reference's start-of-sweep test off(P) < limit (offnorm_kernel), then for
+// every round-robin layer the block solves (solve2_kernel), P <- R^T P R
+// (twoside_kernel) and V <- V R (apply_kernel on Vc).
+static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, int npad, double limit, double tau,
+                               int max_sweeps, int inner_max, char* ws, int* sweeps_out, int64_t* rot_out,
+                               double* off_out, int* inner_cap_out, double* ms_out) {
+    cudaStream_t st = ctx->stream;
+    const int nb = npad / BW;
+    const int npairs = nb / 2;
+    const int ntri = npairs * (npairs + 1) / 2;
+    const int sms = ctx->num_sms;
+    int napply = std::max(1, (4 * sms + npairs - 1) / npairs);
+    int rows = ((npad / 64 + napply - 1) / napply) * 64;
+    napply = (npad + rows - 1) / rows;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    char* p = ws;
+    SweepState* stt = reinterpret_cast<SweepState*>(p); p += al(sizeof(SweepState));
+    int* skip = reinterpret_cast<int*>(p); p += al(size_t(npairs) * 4);
+    double* Rg = reinterpret_cast<double*>(p);
+    cudaError_t e = cudaMemsetAsync(stt, 0, sizeof(SweepState), st);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(solve2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(twoside_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTwoSmem);
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: sweep setup");
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: begin capture");
+    offnorm_kernel<<<1, 1024, 0, st>>>(P, npad, n, stt, limit);
+    for (int layer = 0; layer < nb - 1; ++layer) {
+        solve2_kernel<<<npairs, 256, kSolveSmem, st>>>(P, npad, nb, layer, Rg, skip, stt, tau, inner_max);
+        twoside_kernel<<<ntri, 256, kTwoSmem, st>>>(P, npad, nb, layer, Rg, skip, stt);
+        apply_kernel<<<dim3(npairs, napply), 256, kApplySmem, st>>>(Vc, npad, nb, layer, rows, Rg, skip, stt);
+    }
+    sweep_end_kernel<<<1, 1, 0, st>>>(stt, -1.0);
+    cudaError_t e2 = cudaGetLastError();
+    e = cudaStreamEndCapture(st, &graph);
+    if (e2 != cudaSuccess || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return lsvd_ctx_cuda(ctx, e2 != cudaSuccess ? e2 : e, "large: sweep capture");
+    }
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: graph instantiate");
+    const int launches_per_sweep = 3 * (nb - 1) + 2;
+    SweepState* hst = static_cast<SweepState*>(lsvd_ctx_pinned(ctx, 2 * sizeof(SweepState)));
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    lsvd_status out = LSVD_OK;
+    if (!hst) out = lsvd_ctx_fail(ctx, LSVD_OUT_OF_MEMORY, "large: pinned state");
+    for (int i = 0; i < 2 && out == LSVD_OK; ++i)
+        if ((e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming)) != cudaSuccess)
+            out = lsvd_ctx_cuda(ctx, e, "large: events");
+    EventTimer tm;
+    tm.start(st);
+    int launched = 0;
+    // one sweep ahead of the flag the host reads (see run_sweeps)
+    while (out == LSVD_OK && launched < max_sweeps + 1) {
+        const int k = launched;
+        if ((e = cudaGraphLaunch(exec, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(&hst[k & 1], stt, sizeof(SweepState), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaEventRecord(ev[k & 1], st)) != cudaSuccess) {
+            out = lsvd_ctx_cuda(ctx, e, "large: sweep launch");
+            break;
+        }
+        ++launched;
+        ctx->launches += launches_per_sweep;
+        if (k >= 1) {
+            if ((e = cudaEventSynchronize(ev[(k - 1) & 1])) != cudaSuccess) {
+                out = lsvd_ctx_cuda(ctx, e, "large: sweep sync");
+                break;
+            }
+            if (hst[(k - 1) & 1].converged) break;
+        }
+    }
+    tm.stop(st);
+    SweepState hs;
+    std::memset(&hs, 0, sizeof(hs));
+    if (out == LSVD_OK) {
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+            out = lsvd_ctx_cuda(ctx, e, "large: sweep state");
+        else
+            hs = hst[(launched - 1) & 1];
+    }
+    for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+    cudaGraphExecDestroy(exec);
+    if (out != LSVD_OK) return out;
+    *sweeps_out = hs.sweeps;
+    *rot_out = int64_t(hs.rotations);
+    *off_out = hs.last_off;
+    *inner_cap_out = hs.inner_cap;
+    *ms_out = tm.ms();
+    return hs.converged ? LSVD_OK : LSVD_NOT_CONVERGED;
+}
+
+static size_t sweep_ws_bytes(int gpad, int npad, int num_sms) {
+    const int nb = npad / BW, npairs = nb / 2;
+    const int nchunk = std::max(1, std::min(gpad / 64, (3 * num_sms + npairs - 1) / npairs));
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    return al(sizeof(SweepState)) + al(size_t(npairs) * 4) + al(size_t(npairs) * PW * PW * 8) +
+           al(size_t(npairs) * (nchunk + 1) * PW * PW * 8);
+}
+
+static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,
+                              bool transpose_in, double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
+                              lsvd_precision precision, lsvd_large_info* info, lsvd_diag* diag, bool want_diag) {
+    cudaStream_t st = ctx->stream;
+    cudaError_t e;
+    const int64_t ld = (n + 7) & ~int64_t(7);
+    const int gpad = int((n + 63) & ~int64_t(63));  // G = P is n x n on this route
+    const int npad = gpad;
+    const int64_t ldh = int64_t(gpad) + npad;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t b_a = al(size_t(m) * ld * 8), b_p = al(size_t(ld) * ld * 8), b_h = al(size_t(npad) * ldh * 8);
+    const size_t b_u = al(size_t(m) * ld * 8), b_v = al(size_t(ld) * ld * 8);
+    const size_t b_misc = al(4096 * 8 + 64) + al(size_t(n) * 8) + al(size_t(n) * 4);
+    const size_t b_sw = sweep_ws_bytes(gpad, npad, ctx->num_sms);
+    char* ws = static_cast<char*>(ctx->ws_large.get(b_a + b_p + b_h + b_u + b_v + b_misc + b_sw, &e));
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: workspace");
+    char* p = ws;
+    double* A64 = reinterpret_cast<double*>(p); p += b_a;
+    double* Pm = reinterpret_cast<double*>(p); p += b_p;
+    double* H = reinterpret_cast<double*>(p); p += b_h;
+    double* Ud = reinterpret_cast<double*>(p); p += b_u;
+    double* Vd = reinterpret_cast<double*>(p); p += b_v;
+    double* part = reinterpret_cast<double*>(p);
+    double* dsum = part + 4096;
+    p += al(4096 * 8 + 64);
+    double* sig = reinterpret_cast<double*>(p); p += al(size_t(n) * 8);
+    int* perm_d = reinterpret_cast<int*>(p); p += al(size_t(n) * 4);
+    char* sw = p;
+    // A (m x n) into A64 with an even leading dimension (transposed input: A is n x m)
+    if ((e = cudaMemsetAsync(A64, 0, size_t(m) * ld * 8, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: clear A");
+    if (!transpose_in) {
+        e = cudaMemcpy2DAsync(A64, size_t(ld) * 8, A, size_t(lda) * 8, size_t(n) * 8, size_t(m), cudaMemcpyDefault, st);
+    } else {
+        // A given as n x m (lda): stage it in Ud (n x ldm), then transpose on the device
+        const int64_t ldm = (m + 7) & ~int64_t(7);
+        e = cudaMemcpy2DAsync(Ud, size_t(ldm) * 8, A, size_t(lda) * 8, size_t(m) * 8, size_t(n), cudaMemcpyDefault, st);
+        if (e == cudaSuccess) {
+            transpose_kernel<<<dim3(32, 32), 256, 0, st>>>(int(n), int(m), Ud, ldm, A64, ld);
+            e = cudaGetLastError();
+            ctx->launches += 1;
+        }
+    }
+    if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: copy A");
+    frob2_part_kernel<<<1024, 256, 0, st>>>(int(m), int(n), A64, ld, part);
+    sum_parts_kernel<<<1, 256, 0, st>>>(1024, part, dsum);
+    double f2 = 0.0;
+    if ((e = cudaMemcpyAsync(&f2, dsum, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: norm");
+    if (!std::isfinite(f2)) return lsvd_ctx_fail(ctx, LSVD_NONFINITE_INPUT, "large: non-finite input");
+    lsvd_large_info li;
+    std::memset(&li, 0, sizeof(li));
+    EventTimer total;
+    total.start(st);
+    int32_t mflags = 0;
+    // 1. polar factor Q (m x n, ldq)
+    lsvd_polar_info pinfo;
+    std::memset(&pinfo, 0, sizeof(pinfo));
+    double* X = nullptr;
+    int64_t ldx = 0;
+    EventTimer tpol;
+    tpol.start(st);
+    lsvd_status pst = LSVD_OK;
+    if (f2 > 0.0) {
+        pst = lsvd_polar_run(ctx, m, n, A64, ld, LSVD_PREC_FP64, 120, &X, &ldx, &pinfo);
+        if (pst != LSVD_OK && pst != LSVD_NOT_CONVERGED) return pst;
+    }
+    tpol.stop(st);
+    if (pst == LSVD_NOT_CONVERGED) mflags |= LSVD_MAT_NS_CAP;
+    if (f2 > 0.0 && pinfo.orth > 1e-8 * std::sqrt(double(n))) mflags |= LSVD_MAT_POLAR_UNTRUSTED;
+    li.ns_iters_fp64 = pinfo.iters_fp64;
+    li.flops_fp64 += pinfo.flops_fp64;
+    // scale G so that ||P||_F = ||A||_F is near 1 (a power of two: exact)
+    const double scale = f2 > 0.0 ? std::ldexp(1.0, -std::ilogb(std::sqrt(f2))) : 1.0;
+    int sweeps = 0, inner_cap = 0;
+    int64_t rots = 0;
+    double off = 0.0, ms_eig = 0.0;
+    lsvd_status jst = LSVD_OK;
+    double* P2 = H;                       // npad x npad, row-major (the H slot holds both)
+    double* Vc = H + size_t(npad) * npad;  // npad x npad, row j = v_j
+    if (f2 > 0.0) {
+        // 2. P = Q^T A (n x n); P2 = scale sym(P), Vc = I
+        if ((e = lsvd::dg::dgemm(st, true, false, int(n), int(n), int(m), 1.0, X, ldx, A64, ld, 0.0, Pm, ld)) !=
+            cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "large: P = Q^T A");
+        li.flops_fp64 += 2.0 * double(m) * double(n) * double(n);
+        fill_p2v_kernel<<<2048, 256, 0, st>>>(Pm, ld, int(n), scale, P2, Vc, npad);
+        frob2_part_kernel<<<1024, 256, 0, st>>>(int(n), int(n), P2, npad, part);
+        sum_parts_kernel<<<1, 256, 0, st>>>(1024, part, dsum);
+        ctx->launches += 4;
+        double p2 = 0.0;
+        if ((e = cudaMemcpyAsync(&p2, dsum, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "large: ||P||");
+        // 3. eigenvectors of P by blocked two-sided Jacobi: the reference's
+        //    stop test off(P) < 1e-13 ||P||_F at every sweep start
+        //    (src/lie_svd_small.rs:216-228); rotations of |a_pq| above the
+        //    rounding level eps ||P||_F / sqrt(n) of the entries
+        const double refn = std::max(std::sqrt(p2), 1e-300);
+        const double tau = 2.220446049250313e-16 * refn / std::sqrt(double(npad));
+        jst = run_sweeps2(ctx, P2, Vc, int(n), npad, 1e-13 * refn, tau, 40, 8, sw, &sweeps, &rots, &off,
+                          &inner_cap, &ms_eig);
+        if (jst != LSVD_OK && jst != LSVD_NOT_CONVERGED) return jst;
+        if (jst == LSVD_NOT_CONVERGED) mflags |= LSVD_MAT_JACOBI_CAP;
+        off /= scale;
+        // per sweep and layer: R_a^T P_ab R_b over the block-pair triangle, and V R
+        const double np2 = double(npad / PW);
+        li.flops_fp64 += double(sweeps) * double(npad / BW - 1) *
+                         (np2 * (np2 + 1) / 2 * 4.0 * PW * PW * PW + np2 * 2.0 * PW * PW * npad);
+        // 4. eigenvalues: Rayleigh quotients of the original P for the converged basis
+        if ((e = lsvd::dg::dgemm(st, false, true, int(n), int(n), int(n), 1.0, Vc, npad, Pm, ld, 0.0, Ud, ld)) !=
+            cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "large: P V");
+        li.flops_fp64 += 2.0 * double(n) * double(n) * double(n);
+        rayleigh_kernel<<<(int(n) * 32 + 255) / 256, 256, 0, st>>>(Vc, npad, Ud, ld, int(n), sig);
+        ctx->launches += 2;
+    } else {
+        // A = 0: sigma = 0, V = I, U = the first n columns of I (MGS fill of zero seeds)
+        fill_p2v_kernel<<<2048, 256, 0, st>>>(Pm, ld, 0, 0.0, P2, Vc, npad);
+        if ((e = cudaMemsetAsync(sig, 0, size_t(n) * 8, st)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "large: zero sigma");
+        ctx->launches += 1;
+    }
+    // sigma = max(lambda, 0) in descending eigenvalue order (src/lie_svd_small.rs:270-284, :311)
+    std::vector<double> hs(static_cast<size_t>(n));
+    if ((e = cudaMemcpyAsync(hs.data(), sig, size_t(n) * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: sigma");
+    std::vector<int> perm(static_cast<size_t>(n));
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return hs[a] > hs[b]; });
+    std::vector<double> hsorted(static_cast<size_t>(n));
+    for (int64_t k = 0; k < n; ++k) hsorted[size_t(k)] = std::max(hs[size_t(perm[size_t(k)])], 0.0);
+    if ((e = cudaMemcpyAsync(perm_d, perm.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: perm");
+    gather_vt_kernel<<<2048, 256, 0, st>>>(Vc, npad, 0, int(n), perm_d, Vd, ld);
+    if (f2 > 0.0) {
+        if ((e = lsvd::dg::dgemm(st, false, true, int(m), int(n), int(n), 1.0, X, ldx, Vd, ld, 0.0, Ud, ld)) !=
+            cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "large: U = Q V");
+        li.flops_fp64 += 2.0 * double(m) * double(n) * double(n);
+    } else {
+        std::vector<double> eye(size_t(m) * ld, 0.0);
+        for (int64_t i = 0; i < n; ++i) eye[size_t(i) * ld + i] = 1.0;
+        if ((e = cudaMemcpyAsync(Ud, eye.data(), eye.size() * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "large: U");
+    }
+    ctx->launches += 3;
+    total.stop(st);
+    // 5. outputs: the thin SVD of A, or of A^T for a transposed input (U and Vt swap roles)
+    double* dS = sig;  // sorted sigma back to the device for the diagnostics
+    if ((e = cudaMemcpyAsync(dS, hsorted.data(), size_t(n) * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: sorted sigma");
+    if (want_diag || diag) {
+        double o_u = 0.0, o_v = 0.0, rec = 0.0;
+        auto norm2 = [&](double* out) -> cudaError_t {
+            sum_parts_kernel<<<1, 256, 0, st>>>(1024, part, dsum);
+            cudaError_t ee = cudaMemcpyAsync(out, dsum, 8, cudaMemcpyDeviceToHost, st);
+            return ee == cudaSuccess ? cudaStreamSynchronize(st) : ee;
+        };
+        if (want_diag) {
+            // ||U^T U - I||, ||Vt Vt^T - I||, ||U S Vt - A|| / ||A|| with the GEMMs of this file
+            if ((e = lsvd::dg::dgemm(st, true, false, int(n), int(n), int(m), 1.0, Ud, ld, Ud, ld, 0.0, Pm, ld)) !=
+                cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: diag");
+            diff2_kernel<<<1024, 256, 0, st>>>(int(n), int(n), Pm, ld, nullptr, 0, part);
+            if ((e = norm2(&o_u)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: diag");
+            if ((e = lsvd::dg::dgemm(st, false, true, int(n), int(n), int(n), 1.0, Vd, ld, Vd, ld, 0.0, Pm, ld)) !=
+                cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: diag");
+            diff2_kernel<<<1024, 256, 0, st>>>(int(n), int(n), Pm, ld, nullptr, 0, part);
+            if ((e = norm2(&o_v)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: diag");
+            // U diag(S) in X's slot (Q is no longer needed once U = Q V is formed), then
+            // A64 <- U S Vt - A64 and its sum of squares
+            if (X) {
+                scale_cols_kernel<<<2048, 256, 0, st>>>(int(m), int(n), Ud, ld, dS, X, ld);
+                if ((e = lsvd::dg::dgemm(st, false, false, int(m), int(n), int(n), 1.0, X, ld, Vd, ld, -1.0, A64,
+                                         ld)) != cudaSuccess)
+                    return lsvd_ctx_cuda(ctx, e, "large: diag");
+            }
+            frob2_part_kernel<<<1024, 256, 0, st>>>(int(m), int(n), A64, ld, part);
+            if ((e = norm2(&rec)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: diag");
+            ctx->launches += 10;
+            o_u = std::sqrt(o_u);
+            o_v = std::sqrt(o_v);
+            rec = f2 > 0.0 ? std::sqrt(rec / f2) : 0.0;
+        }
+        if (diag) {
+            diag->rel_recon = rec;
+            diag->orth_u = transpose_in ? o_v : o_u;
+            diag->orth_v = transpose_in ? o_u : o_v;
+            diag->ns_iters = pinfo.iters_fp64;
+            diag->jacobi_sweeps = f2 > 0.0 ? sweeps + 1 : 0;  // + the sweep whose start test stopped the solve
+            diag->rotations = rots;
+            diag->flags = mflags;
+            diag->route = LSVD_ROUTE_SMALL;
+        }
+    }
+    if (!transpose_in) {
+        if ((e = cudaMemcpy2DAsync(U, size_t(ldu) * 8, Ud, size_t(ld) * 8, size_t(n) * 8, size_t(m), cudaMemcpyDefault,
+                                   st)) != cudaSuccess ||
+            (e = cudaMemcpy2DAsync(Vt, size_t(ldvt) * 8, Vd, size_t(ld) * 8, size_t(n) * 8, size_t(n),
+                                   cudaMemcpyDefault, st)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "large: copy out");
+    } else {
+        // A^T = U S Vt  =>  A = Vt^T S U^T: the caller's U (n x n) = Vd^T and Vt (n x m) = Ud^T,
+        // transposed on the device into the free P and A64 slots
+        const int64_t ldm = (m + 7) & ~int64_t(7);
+        transpose_kernel<<<dim3(32, 32), 256, 0, st>>>(int(n), int(n), Vd, ld, Pm, ld);
+        transpose_kernel<<<dim3(32, 32), 256, 0, st>>>(int(m), int(n), Ud, ld, A64, ldm);
+        ctx->launches += 2;
+        if ((e = cudaGetLastError()) != cudaSuccess ||
+            (e = cudaMemcpy2DAsync(U, size_t(ldu) * 8, Pm, size_t(ld) * 8, size_t(n) * 8, size_t(n),
+                                   cudaMemcpyDefault, st)) != cudaSuccess ||
+            (e = cudaMemcpy2DAsync(Vt, size_t(ldvt) * 8, A64, size_t(ldm) * 8, size_t(m) * 8, size_t(n),
+                                   cudaMemcpyDefault, st)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "large: copy out");
+    }
+    if ((e = cudaMemcpyAsync(S, hsorted.data(), size_t(n) * 8, cudaMemcpyDefault, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: copy S");
+    li.sweeps_fp64 = sweeps;
+    li.rotations = rots;
+    li.flags = mflags;
+    li.last_offdiag = off;
+    li.inner_cap_pairs = inner_cap;
+    li.ms_polar = tpol.ms();
+    li.ms_eig_fp64 = ms_eig;
+    li.ms_total = total.ms();
+    if (diag) {
+        li.rel_recon = diag->rel_recon;
+        li.orth_u = diag->orth_u;
+        li.orth_v = diag->orth_v;
+    }
+    if (info) *info = li;
+    (void)precision;
+    if (jst == LSVD_NOT_CONVERGED || pst == LSVD_NOT_CONVERGED) return LSVD_NOT_CONVERGED;
+    return LSVD_OK;
+}
+
+lsvd_status lsvd_large_solve(lsvd_context* ctx, int64_t rows, int64_t cols, const double* A, int64_t lda,
+                             double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
+                             lsvd_precision precision, lsvd_large_info* info, lsvd_diag* diag, bool want_diag) {
+    // wide inputs run on A^T (the reference transposes, src/lie_svd_small.rs:343-348)
+    const bool tr = cols > rows;
+    const int64_t m = tr ? cols : rows, n = tr ? rows : cols;
+    return large_impl(ctx, m, n, A, lda, tr, U, ldu, S, Vt, ldvt, precision, info, diag, want_diag);
+}
+
+extern "C" lsvd_status lsvd_svd_large_f64(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,
+                                          double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
+                                          lsvd_precision precision, lsvd_large_info* info, uint32_t flags) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    if (m < 1 || n < 1) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "lsvd_svd_large_f64: empty matrix");
+    const int64_t k = std::min(m, n);
+    if (!A || !U || !S || !Vt || lda < n || ldu < k || ldvt < n)
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_svd_large_f64: bad pointer or leading dimension");
+    if (std::max(m, n) > (int64_t(1) << 16) || k > 16384)
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "lsvd_svd_large_f64: larger than 65536 x 16384");
+    if (precision != LSVD_PREC_FP64)
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "lsvd_svd_large_f64: precision");
+    cudaSetDevice(ctx->device);
+    lsvd_diag d;
+    return lsvd_large_solve(ctx, m, n, A, lda, U, ldu, S, Vt, ldvt, precision, info, &d,
+                            (flags & LSVD_WANT_DIAG) != 0);
+}

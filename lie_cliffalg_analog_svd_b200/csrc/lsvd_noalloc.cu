@@ -1,20 +1,18 @@
 // lsvd_noalloc.cu -- the batched FP64 SVD for callers that cannot allocate.
 //
 // Some callers may not allocate device memory at the point where they need
-// an SVD: code that runs while its CUDA stream is being captured into a graph
-// (cudaMalloc is not permitted during capture), real-time loops where the
-// implicit device synchronisation of cudaMalloc/cudaFree would stall other
-// streams, and hosts whose device memory is owned by their own pool or
-// allocator (a framework arena, a Rust or JVM runtime handing out
-// preallocated buffers) and must not see a second allocator.
-// lsvd_svd_batched_noalloc_f64 serves them: the caller passes device buffers
-// for the inputs and outputs, and every piece of working memory the solve
-// needs (the work queue head, outcome flags, the per-size schedule and the
-// micro->small escalation list) lives in one file-scope device array,
-// g_noalloc_scratch, of LSVD_NOALLOC_SCRATCH_BYTES.  That array is part of
-// the library image: every GPU that loads the library holds it until the
-// process exits.  The schedule is built on the device by a setup kernel, so
-// no host or device memory is allocated on any call.
+// an SVD: real-time loops where the implicit device synchronisation of
+// cudaMalloc/cudaFree would stall other streams, and hosts whose device
+// memory is owned by their own pool or allocator (a framework arena, a Rust
+// or JVM runtime handing out preallocated buffers) and must not see a second
+// allocator.  lsvd_svd_batched_noalloc_f64 serves them: the caller passes
+// device buffers for the inputs and outputs, and every piece of working
+// memory the solve needs (the work queue head, outcome flags, the per-size
+// schedule and the micro->small escalation list) lives in one file-scope
+// device array, g_noalloc_scratch, of LSVD_NOALLOC_SCRATCH_BYTES.  That array
+// is part of the library image: every GPU that loads the library holds it
+// until the process exits.  The schedule is built on the device by a setup
+// kernel, so no host or device memory is allocated on any call.
 //
 // All calls share the one array.  Calls whose work overlaps on a GPU (two
 // streams, or two host threads, at the same time on the same device) race on
@@ -49,9 +47,10 @@ struct ClassCfgArray {
     int per_item[kMaxClasses];
 };
 
-// header layout (ints): head, fb_count, agg, n_items, hist[65], start[65]
+// header layout (ints): head, fb_count, agg, n_items, bad_n, hist[65], start[65]
 struct Header {
     int head, fb_count, agg, n_items;
+    int bad_n;  // sizes outside 1..64 seen on the device (the call then solves nothing)
     int hist[65];
     int start[65];
 };
@@ -96,16 +95,31 @@ __global__ void __launch_bounds__(256, 1)
     Header* h = L.hdr;
     __shared__ int64_t carry_a, carry_s;
     const int tid = threadIdx.x;
+    __shared__ int s_bad;
     if (tid == 0) {
         h->head = 0;
         h->fb_count = 0;
         h->agg = 0;
         h->n_items = 0;
+        h->bad_n = 0;
         carry_a = 0;
         carry_s = 0;
+        s_bad = 0;
     }
     for (int i = tid; i < 65; i += 256) h->hist[i] = 0;
     __syncthreads();
+    // The host checked the sizes when the call was made; with LSVD_ASYNC the
+    // caller's array is only read when the copy runs, so check again here and
+    // solve nothing (n_items = 0) if a size left 1..64 in between.
+    for (int t = tid; t < count; t += 256) {
+        const int v = L.n[t];
+        if (v < 1 || v > kMaxN) atomicOr(&s_bad, 1);
+    }
+    __syncthreads();
+    if (s_bad) {
+        if (tid == 0) h->bad_n = 1;
+        return;
+    }
     for (int t = tid; t < count; t += 256) atomicAdd(&h->hist[L.n[t]], 1);
     // exclusive prefix sums of n^2 and n, chunks of 256
     __shared__ int64_t sa[256], ss[256];
@@ -288,12 +302,32 @@ __global__ void __launch_bounds__(kCtaThreads, 1) noalloc_fallback_kernel(const 
 // symbol is only a stand-in and must never be passed to a kernel), the
 // dynamic shared-memory limit of the persistent kernel and the SM count.
 struct DeviceSetup {
-    std::once_flag once;
-    cudaError_t err = cudaSuccess;
+    std::mutex mu;
+    bool done = false;  // set only by a set-up that succeeded; a failed one is retried
     unsigned char* scratch = nullptr;
     int num_sms = 0;
 };
 DeviceSetup g_setup[64];
+
+// Runs the per-device set-up once it succeeds; returns its error otherwise.
+cudaError_t device_setup(DeviceSetup& ds, int dev, int smem) {
+    std::lock_guard<std::mutex> lock(ds.mu);
+    if (ds.done) return cudaSuccess;
+    void* p = nullptr;
+    cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(noalloc_batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int sms = 0;
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (err != cudaSuccess) {
+        cudaGetLastError();  // leave no pending error behind; the next call retries
+        return err;
+    }
+    ds.scratch = static_cast<unsigned char*>(p);
+    ds.num_sms = sms;
+    ds.done = true;
+    return cudaSuccess;
+}
 
 int noalloc_smem_bytes(const ClassCfg* cls) {
     int mx = 0;
@@ -332,19 +366,10 @@ extern "C" lsvd_status lsvd_svd_batched_noalloc_f64(void* stream, int64_t count,
     }
     const int smem = noalloc_smem_bytes(na.cls);
     DeviceSetup& ds = g_setup[dev];
-    // The first call on a device does the set-up below (symbol address and
-    // kernel attributes); make that first call before any stream capture.
-    std::call_once(ds.once, [&]() {
-        void* p = nullptr;
-        ds.err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (ds.err == cudaSuccess) ds.scratch = static_cast<unsigned char*>(p);
-        if (ds.err == cudaSuccess)
-            ds.err = cudaFuncSetAttribute(noalloc_batched_kernel,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (ds.err == cudaSuccess)
-            ds.err = cudaDeviceGetAttribute(&ds.num_sms, cudaDevAttrMultiProcessorCount, dev);
-    });
-    if (ds.err != cudaSuccess || !ds.scratch) return LSVD_CUDA_ERROR;
+    // The first successful call on a device does the set-up (the device
+    // address of the static array, kernel attributes); a set-up that failed
+    // is tried again on the next call.
+    if (device_setup(ds, dev, smem) != cudaSuccess) return LSVD_CUDA_ERROR;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const Layout L = layout_of(ds.scratch);
     na.base = ds.scratch;
@@ -363,10 +388,12 @@ extern "C" lsvd_status lsvd_svd_batched_noalloc_f64(void* stream, int64_t count,
     noalloc_fallback_kernel<<<fgrid > 0 ? fgrid : 1, kCtaThreads, team_smem_doubles(4, kCtaThreads / 32) * 8, st>>>(na);
     if ((e = cudaGetLastError()) != cudaSuccess) return LSVD_CUDA_ERROR;
     if (flags & LSVD_ASYNC) return LSVD_OK;
-    int agg = 0;
-    if (cudaMemcpyAsync(&agg, &L.hdr->agg, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    int agg_bad[5] = {0, 0, 0, 0, 0};  // head, fb_count, agg, n_items, bad_n
+    if (cudaMemcpyAsync(agg_bad, L.hdr, sizeof(agg_bad), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return LSVD_CUDA_ERROR;
+    const int agg = agg_bad[2];
+    if (agg_bad[4]) return LSVD_BAD_ARGUMENT;
     if (agg & LSVD_MAT_NONFINITE) return LSVD_NONFINITE_INPUT;
     if (agg & LSVD_MAT_JACOBI_CAP) return LSVD_NOT_CONVERGED;
     return LSVD_OK;

@@ -2,8 +2,9 @@
 // (newton_schulz_polar, src/lie_svd_small.rs:158-183, generalised to m >= n)
 // in three precisions:
 //   FP64       : X <- 0.5 X (3I - X^T X) from X0 = A/||A||_F with FP64 GEMMs
-//                (cuBLAS DGEMM: plain library GEMMs) and the reference's
-//                stopping rule (delta < 1e-13 sqrt(n), cap 120);
+//                on the FP64 tensor path (lsvd_dgemm.cuh, mma.sync m8n8k4)
+//                and the reference's stopping rule (delta < 1e-13 sqrt(n),
+//                cap 120);
 //   TF32, BF16 : the same iteration on tensor cores (lsvd_tcgemm.cuh,
 //                tcgen05, FP32 accumulation) until the update reaches the
 //                low-precision floor, then FP64 refinement iterations until
@@ -14,7 +15,6 @@
 // mixed result differs from A's polar factor by about u_lo sqrt(n) in
 // Frobenius norm (u_lo = 2^-11 TF32, 2^-8 BF16), more where A's singular
 // values fall below ~u_lo sigma_1.  The FP64 path has no such floor.
-#include <cublas_v2.h>
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "lsvd.h"
+#include "lsvd_dgemm.cuh"
 #include "lsvd_internal.h"
 #include "lsvd_tcgemm.cuh"
 
@@ -121,7 +122,7 @@ __global__ void sum_kernel(int count, const double* part, double* out) {
     if (threadIdx.x == 0) *out = red[0];
 }
 
-__global__ void frob2_kernel(int m, int n, const double* A, int lda, double* part) {
+__global__ void frob2_kernel(int m, int n, const double* A, int64_t lda, double* part) {
     __shared__ double red[256];
     double s = 0.0;
     const size_t tot = size_t(m) * n;
@@ -138,7 +139,8 @@ __global__ void frob2_kernel(int m, int n, const double* A, int lda, double* par
     if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
-// FP64: X <- 1.5 X - 0.5 Y, squared update norm per block; or X = A/scale.
+// FP64: X <- 1.5 X - 0.5 Y over the whole padded buffer (padding columns are
+// zero in X and Y and stay zero), squared update norm per block.
 __global__ void ns_update64_kernel(size_t count, double* X, const double* Y, double* part) {
     __shared__ double red[256];
     double s = 0.0;
@@ -157,25 +159,32 @@ __global__ void ns_update64_kernel(size_t count, double* X, const double* Y, dou
     if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
-__global__ void scale64_kernel(int m, int n, const double* A, int lda, double inv, double* X) {
-    const size_t tot = size_t(m) * n;
-    for (size_t e = blockIdx.x * size_t(256) + threadIdx.x; e < tot; e += size_t(gridDim.x) * 256)
-        X[e] = A[(e / n) * lda + e % n] * inv;
+// X (m x ld, padding columns zero) = A (m x n, lda) * inv.
+__global__ void scale64_kernel(int m, int n, const double* A, int64_t lda, double inv, double* X, int64_t ld) {
+    const size_t tot = size_t(m) * ld;
+    for (size_t e = blockIdx.x * size_t(256) + threadIdx.x; e < tot; e += size_t(gridDim.x) * 256) {
+        const size_t i = e / ld, j = e % ld;
+        X[e] = j < size_t(n) ? A[i * lda + j] * inv : 0.0;
+    }
 }
 
-__global__ void widen_kernel(size_t count, const float* X32, double* X64) {
-    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < count;
-         e += size_t(gridDim.x) * blockDim.x)
-        X64[e] = double(X32[e]);
+__global__ void widen_kernel(int m, int n, const float* X32, double* X64, int64_t ld) {
+    const size_t tot = size_t(m) * ld;
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < tot;
+         e += size_t(gridDim.x) * blockDim.x) {
+        const size_t i = e / ld, j = e % ld;
+        X64[e] = j < size_t(n) ? double(X32[i * n + j]) : 0.0;
+    }
 }
 
-// ||T - I||_F^2 partials for the orthogonality check of the final iterate.
-__global__ void orth2_kernel(int n, const double* T, double* part) {
+// ||T - I||_F^2 partials (T n x n with leading dimension ld).
+__global__ void orth2_kernel(int n, const double* T, int64_t ld, double* part) {
     __shared__ double red[256];
     double s = 0.0;
     const size_t tot = size_t(n) * n;
     for (size_t e = blockIdx.x * size_t(256) + threadIdx.x; e < tot; e += size_t(gridDim.x) * 256) {
-        const double d = T[e] - ((e / n) == (e % n) ? 1.0 : 0.0);
+        const size_t i = e / n, j = e % n;
+        const double d = T[i * ld + j] - (i == j ? 1.0 : 0.0);
         s += d * d;
     }
     red[threadIdx.x] = s;
@@ -242,17 +251,6 @@ cudaError_t launch_gemm(cudaStream_t st, const void* A, const void* B, float* C,
                         : launch_gemm_t<PREC, kTile>(st, A, B, C, M, N, K, err);
 }
 
-cublasHandle_t blas(lsvd_context* ctx) {
-    if (!ctx->cublas) {
-        cublasHandle_t h;
-        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return nullptr;
-        ctx->cublas = h;
-    }
-    cublasHandle_t h = static_cast<cublasHandle_t>(ctx->cublas);
-    cublasSetStream(h, ctx->stream);
-    return h;
-}
-
 // Start/stop events around the GEMM launches of one iteration; the summed
 // durations are read after the iteration's own synchronisation.
 struct GemmTimer {
@@ -279,10 +277,6 @@ struct GemmTimer {
 };
 
 }  // namespace
-
-void lsvd_destroy_blas(void* h) {
-    if (h) cublasDestroy(static_cast<cublasHandle_t>(h));
-}
 
 extern "C" lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N, int64_t K,
                                          const float* A, const float* B, float* C,
@@ -326,29 +320,41 @@ extern "C" lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N
     return LSVD_OK;
 }
 
-extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, const double* A,
-                                      int64_t lda, double* Q, int64_t ldq, lsvd_precision precision,
-                                      lsvd_polar_info* info, uint32_t flags) {
+extern "C" lsvd_status lsvd_gemm_f64(lsvd_context* ctx, int32_t trans_a, int32_t trans_b, int64_t M,
+                                     int64_t N, int64_t K, double alpha, const double* A, int64_t lda,
+                                     const double* B, int64_t ldb, double beta, double* C, int64_t ldc) {
     if (!ctx) return LSVD_BAD_ARGUMENT;
-    if (m <= 0 || n <= 0 || m < n) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "polar: need m >= n >= 1");
-    if (!A || !Q || lda < n || ldq < n) return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "polar: bad pointer");
+    if (M < 0 || N < 0 || K < 0 || M > (1 << 24) || N > (1 << 24) || K > (1 << 24))
+        return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "lsvd_gemm_f64: bad sizes");
+    if (!A || !B || !C || ldc < N || lda < (trans_a ? M : K) || ldb < (trans_b ? K : N))
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_gemm_f64: bad pointer or leading dimension");
+    if ((lda | ldb) & 1 || (reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15)
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "lsvd_gemm_f64: lda, ldb even and A, B 16-byte aligned");
+    cudaSetDevice(ctx->device);
+    cudaError_t e = lsvd::dg::dgemm(ctx->stream, trans_a != 0, trans_b != 0, int(M), int(N), int(K), alpha, A,
+                                    lda, B, ldb, beta, C, ldc);
+    ctx->launches += 1;
+    return lsvd_ctx_cuda(ctx, e, "lsvd_gemm_f64");
+}
+
+lsvd_status lsvd_polar_run(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,
+                           lsvd_precision precision, int fp64_cap, double** Xout, int64_t* ldx_out,
+                           lsvd_polar_info* info) {
     const bool lowp = precision == LSVD_PREC_MIXED_TF32 || precision == LSVD_PREC_MIXED_BF16;
     if (lowp && (m % kTile || n % kTile))
         return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "polar: TF32/BF16 need m, n multiples of 128");
     if (m * n > (int64_t(1) << 31)) return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "polar: too large");
-    cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
-    cublasHandle_t h = blas(ctx);
-    if (!h) return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "cublasCreate failed");
-    const bool dev = (flags & LSVD_DEVICE_POINTERS) != 0;
-    const size_t mn = size_t(m) * n, nn = size_t(n) * n;
+    const int64_t ld = (n + 7) & ~int64_t(7);  // FP64 buffers: even leading dimension for the GEMMs
+    const size_t mn = size_t(m) * ld, nn = size_t(ld) * ld;
+    const size_t mn32 = size_t(m) * n, nn32 = size_t(n) * n;
     const int prec = precision == LSVD_PREC_MIXED_BF16 ? kBF16 : kTF32;
     const size_t lo = prec == kBF16 ? 2 : 4;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     // workspace: A64 | X64 | Y64 | T64 | part | (X32 | Y32 | T32 | Xlo | Xt | Tlo | err)
     const int nparts = 4096;
     size_t bytes = al(mn * 8) * 3 + al(nn * 8) + al(nparts * 8) + 64;
-    if (lowp) bytes += al(mn * 4) * 2 + al(nn * 4) + al(mn * lo) * 2 + al(nn * lo) + 64;
+    if (lowp) bytes += al(mn32 * 4) * 2 + al(nn32 * 4) + al(mn32 * lo) * 2 + al(nn32 * lo) + 64;
     cudaError_t e;
     char* ws = static_cast<char*>(ctx->ws_polar.get(bytes, &e));
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar workspace");
@@ -359,7 +365,13 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
     double* T64 = reinterpret_cast<double*>(p); p += al(nn * 8);
     double* part = reinterpret_cast<double*>(p); p += al(nparts * 8);
     double* dsum = reinterpret_cast<double*>(p); p += 64;
-    if ((e = cudaMemcpy2DAsync(A64, size_t(n) * 8, A, size_t(lda) * 8, size_t(n) * 8, size_t(m),
+    // padding columns of the FP64 buffers must read as zero: the GEMMs write
+    // only the n valid columns, and the update and its norm run over the
+    // whole padded buffer
+    if ((e = cudaMemsetAsync(Y64, 0, mn * 8, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(T64, 0, nn * 8, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(A64, 0, mn * 8, st)) != cudaSuccess ||
+        (e = cudaMemcpy2DAsync(A64, size_t(ld) * 8, A, size_t(lda) * 8, size_t(n) * 8, size_t(m),
                                cudaMemcpyDefault, st)) != cudaSuccess)
         return lsvd_ctx_cuda(ctx, e, "polar copy A");
     const double refn = std::sqrt(double(n));
@@ -369,30 +381,29 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
         if (ee == cudaSuccess) ee = cudaStreamSynchronize(st);
         return ee;
     };
-    frob2_kernel<<<1024, 256, 0, st>>>(int(m), int(n), A64, int(n), part);
+    frob2_kernel<<<1024, 256, 0, st>>>(int(m), int(n), A64, ld, part);
     double f2 = 0.0;
     if ((e = read_sum(1024, &f2)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar norm");
     const double inv = 1.0 / std::max(std::sqrt(f2), 1e-300);
     int it_lo = 0, it_hi = 0;
     double flops_lo = 0.0, flops_hi = 0.0;
     GemmTimer tlo, thi;
-    const double one = 1.0, zero = 0.0;
     if (lowp) {
-        float* X32 = reinterpret_cast<float*>(p); p += al(mn * 4);
-        float* Y32 = reinterpret_cast<float*>(p); p += al(mn * 4);
-        float* T32 = reinterpret_cast<float*>(p); p += al(nn * 4);
-        void* Xlo = p; p += al(mn * lo);
-        void* Xt = p; p += al(mn * lo);
-        void* Tlo = p; p += al(nn * lo);
+        float* X32 = reinterpret_cast<float*>(p); p += al(mn32 * 4);
+        float* Y32 = reinterpret_cast<float*>(p); p += al(mn32 * 4);
+        float* T32 = reinterpret_cast<float*>(p); p += al(nn32 * 4);
+        void* Xlo = p; p += al(mn32 * lo);
+        void* Xt = p; p += al(mn32 * lo);
+        void* Tlo = p; p += al(nn32 * lo);
         int* err = reinterpret_cast<int*>(p);
         cudaMemsetAsync(err, 0, 4, st);
         const dim3 ug(unsigned(n / 32), unsigned(m / 32));
         const int nub = int(ug.x * ug.y);
         double* upart = Y64;  // Y64 is unused in the low-precision phase: 2 partials per block
         if (prec == kBF16)
-            ns_update_kernel<kBF16><<<ug, 256, 0, st>>>(int(m), int(n), X32, nullptr, A64, int(n), inv, Xlo, Xt, upart);
+            ns_update_kernel<kBF16><<<ug, 256, 0, st>>>(int(m), int(n), X32, nullptr, A64, int(ld), inv, Xlo, Xt, upart);
         else
-            ns_update_kernel<kTF32><<<ug, 256, 0, st>>>(int(m), int(n), X32, nullptr, A64, int(n), inv, Xlo, Xt, upart);
+            ns_update_kernel<kTF32><<<ug, 256, 0, st>>>(int(m), int(n), X32, nullptr, A64, int(ld), inv, Xlo, Xt, upart);
         // Stop the low-precision phase when the relative update
         // delta/||X||_F reaches a few units of the low precision: beyond it
         // the iterate only moves by rounding noise, and from there the FP64
@@ -404,7 +415,7 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
                 tlo.mark(0, st);
                 e = launch_gemm<kBF16>(st, Xt, Xt, T32, int(n), int(n), int(m), err);
                 tlo.mark(1, st);
-                if (e == cudaSuccess) to_lo_kernel<kBF16><<<1024, 256, 0, st>>>(nn, T32, Tlo);
+                if (e == cudaSuccess) to_lo_kernel<kBF16><<<1024, 256, 0, st>>>(nn32, T32, Tlo);
                 tlo.mark(2, st);
                 if (e == cudaSuccess) e = launch_gemm<kBF16>(st, Xlo, Tlo, Y32, int(m), int(n), int(n), err);
                 tlo.mark(3, st);
@@ -414,7 +425,7 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
                 tlo.mark(0, st);
                 e = launch_gemm<kTF32>(st, Xt, Xt, T32, int(n), int(n), int(m), err);
                 tlo.mark(1, st);
-                if (e == cudaSuccess) to_lo_kernel<kTF32><<<1024, 256, 0, st>>>(nn, T32, Tlo);
+                if (e == cudaSuccess) to_lo_kernel<kTF32><<<1024, 256, 0, st>>>(nn32, T32, Tlo);
                 tlo.mark(2, st);
                 if (e == cudaSuccess) e = launch_gemm<kTF32>(st, Xlo, Tlo, Y32, int(m), int(n), int(n), err);
                 tlo.mark(3, st);
@@ -438,27 +449,27 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
             if (!std::isfinite(d2x2[0]) || !std::isfinite(d2x2[1])) break;
             if (std::sqrt(d2x2[0]) < floor_rel * std::sqrt(d2x2[1])) break;
         }
-        widen_kernel<<<2048, 256, 0, st>>>(mn, X32, X64);
+        widen_kernel<<<2048, 256, 0, st>>>(int(m), int(n), X32, X64, ld);
+        if ((e = cudaMemsetAsync(Y64, 0, mn * 8, st)) != cudaSuccess)  // held the partials
+            return lsvd_ctx_cuda(ctx, e, "polar clear Y");
     } else {
-        scale64_kernel<<<2048, 256, 0, st>>>(int(m), int(n), A64, int(n), inv, X64);
+        scale64_kernel<<<2048, 256, 0, st>>>(int(m), int(n), A64, ld, inv, X64, ld);
     }
-    // FP64 iterations (refinement, or the whole FP64 iteration): cuBLAS works
-    // column-major, so the row-major X (m x n) is the column-major X^T (n x m).
+    // FP64 iterations (refinement, or the whole FP64 iteration) on the FP64
+    // tensor path: T = X^T X (K = m), Y = X T (K = n), row-major throughout.
     bool conv = false;
-    const int cap = lowp ? 120 - it_lo : 120;
+    const int cap = std::min(fp64_cap, lowp ? 120 - it_lo : 120);
     for (int it = 0; it < cap; ++it) {
-        // T = X^T X  ->  col-major: X^T (n x m) * (X^T)^T
         thi.mark(0, st);
-        const bool g1 = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, int(n), int(n), int(m), &one, X64, int(n),
-                                    X64, int(n), &zero, T64, int(n)) == CUBLAS_STATUS_SUCCESS;
+        e = lsvd::dg::dgemm(st, true, false, int(n), int(n), int(m), 1.0, X64, ld, X64, ld, 0.0, T64, ld);
         thi.mark(1, st);
         thi.mark(2, st);
-        const bool g2 = g1 && cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, int(n), int(m), int(n), &one, T64,
-                                          int(n), X64, int(n), &zero, Y64, int(n)) == CUBLAS_STATUS_SUCCESS;
+        if (e == cudaSuccess)
+            e = lsvd::dg::dgemm(st, false, false, int(m), int(n), int(n), 1.0, X64, ld, T64, ld, 0.0, Y64, ld);
         thi.mark(3, st);
-        if (!g2) return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "cublasDgemm failed");
+        if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar fp64 gemm");
         ns_update64_kernel<<<nparts, 256, 0, st>>>(mn, X64, Y64, part);
-        ctx->launches += 1;
+        ctx->launches += 3;
         double d2 = 0.0;
         if ((e = read_sum(nparts, &d2)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar fp64 sync");
         thi.accumulate();
@@ -472,15 +483,13 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
         }
     }
     // orthogonality of the returned factor: ||X^T X - I||_F
-    cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, int(n), int(n), int(m), &one, X64, int(n), X64, int(n), &zero,
-                T64, int(n));
-    orth2_kernel<<<nparts, 256, 0, st>>>(int(n), T64, part);
+    if ((e = lsvd::dg::dgemm(st, true, false, int(n), int(n), int(m), 1.0, X64, ld, X64, ld, 0.0, T64, ld)) !=
+        cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "polar orth gemm");
+    orth2_kernel<<<nparts, 256, 0, st>>>(int(n), T64, ld, part);
+    ctx->launches += 2;
     double o2 = 0.0;
     if ((e = read_sum(nparts, &o2)) != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "polar orth");
-    if ((e = cudaMemcpy2DAsync(Q, size_t(ldq) * 8, X64, size_t(n) * 8, size_t(n) * 8, size_t(m),
-                               cudaMemcpyDefault, st)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(st)) != cudaSuccess)
-        return lsvd_ctx_cuda(ctx, e, "polar copy out");
     if (info) {
         info->iters_lowp = it_lo;
         info->iters_fp64 = it_hi;
@@ -492,5 +501,29 @@ extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, c
         info->converged = conv ? 1 : 0;
         info->pad_ = 0;
     }
+    *Xout = X64;
+    *ldx_out = ld;
     return conv ? LSVD_OK : LSVD_NOT_CONVERGED;
+}
+
+extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, const double* A,
+                                      int64_t lda, double* Q, int64_t ldq, lsvd_precision precision,
+                                      lsvd_polar_info* info, uint32_t flags) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    if (m <= 0 || n <= 0 || m < n) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "polar: need m >= n >= 1");
+    if (!A || !Q || lda < n || ldq < n) return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "polar: bad pointer");
+    if (precision != LSVD_PREC_FP64 && precision != LSVD_PREC_MIXED_TF32 && precision != LSVD_PREC_MIXED_BF16)
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "polar: unknown precision");
+    (void)flags;  // host and device pointers are both handled by cudaMemcpy2DAsync's default kind
+    cudaSetDevice(ctx->device);
+    double* X = nullptr;
+    int64_t ldx = 0;
+    const lsvd_status st = lsvd_polar_run(ctx, m, n, A, lda, precision, 120, &X, &ldx, info);
+    if (st != LSVD_OK && st != LSVD_NOT_CONVERGED) return st;
+    cudaError_t e;
+    if ((e = cudaMemcpy2DAsync(Q, size_t(ldq) * 8, X, size_t(ldx) * 8, size_t(n) * 8, size_t(m),
+                               cudaMemcpyDefault, ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "polar copy out");
+    return st;
 }

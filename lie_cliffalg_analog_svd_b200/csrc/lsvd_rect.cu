@@ -92,10 +92,28 @@ extern "C" lsvd_status lsvd_small_solve_rectangular_f64(lsvd_context* ctx, int64
     if (m <= 0 || d <= 0)
         return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "LieSvdSmall::solve_rectangular: empty input");
     const int64_t k = m < d ? m : d;
-    if (k > lsvd::kMaxN || (m > d ? m : d) > (int64_t(1) << 24))
-        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "solve_rectangular: min(m, d) must be <= 64");
     if (!A || !U || !S || !Vt || lda < d || ldu < k || ldvt < d)
         return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "solve_rectangular: bad pointer or leading dimension");
+    if (k > lsvd::kMaxN) {
+        // beyond the shared-memory kernels: the thin route of the large solve
+        if (k > 16384 || (m > d ? m : d) > (int64_t(1) << 16))
+            return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "solve_rectangular: larger than 65536 x 16384");
+        cudaSetDevice(ctx->device);
+        lsvd_diag hd;
+        const lsvd_status st = lsvd_large_solve(ctx, m, d, A, lda, U, ldu, S, Vt, ldvt, LSVD_PREC_FP64, nullptr,
+                                                &hd, (flags & LSVD_WANT_DIAG) != 0);
+        if (diag && st != LSVD_CUDA_ERROR && st != LSVD_OUT_OF_MEMORY && st != LSVD_NONFINITE_INPUT) {
+            if (flags & LSVD_DEVICE_POINTERS) {
+                if (cudaMemcpy(diag, &hd, sizeof(hd), cudaMemcpyHostToDevice) != cudaSuccess)
+                    return lsvd_ctx_fail(ctx, LSVD_CUDA_ERROR, "copy diag out");
+            } else {
+                *diag = hd;
+            }
+        }
+        return st;
+    }
+    if ((m > d ? m : d) > (int64_t(1) << 24))
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "solve_rectangular: too many rows");
     if (m == d)
         return lsvd_single_small(ctx, m, A, lda, U, ldu, S, Vt, ldvt, diag, nullptr, 0, nullptr,
                                  nullptr, flags, 0, false);

@@ -17,7 +17,9 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <atomic>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -921,6 +923,40 @@ int oracle_fmt_e17(double x, char* buf, int64_t cap) {
         std::snprintf(buf, size_t(cap), "%s", s.c_str());
     }
     return int(s.size());
+}
+
+// Batch driver of the timed CPU baseline (no reference counterpart: the
+// reference solves one matrix per call).  Matrices idx[0..count) of a packed
+// uneven batch -- matrix t is n[t] x n[t] at element offset aoff[t], its
+// singular values at soff[t] -- are solved by `threads` std::threads pulling
+// positions from one atomic counter, each with the route of LieSvd::solve's
+// exact tiers (LieSvdMicro for n <= 4, src/lie_svd_adaptive.rs:105-106,
+// LieSvdSmall otherwise).  Outputs land at the same offsets.  Returns the
+// number of matrices solved.
+int64_t oracle_svd_batch(int64_t count, const int32_t* idx, const int32_t* n, const int64_t* aoff,
+                         const int64_t* soff, const double* A, double* U, double* S, double* Vt,
+                         int32_t threads) {
+    std::atomic<int64_t> next{0};
+    std::atomic<int64_t> done{0};
+    auto worker = [&]() {
+        oracle_small_info info;
+        for (;;) {
+            const int64_t k = next.fetch_add(1);
+            if (k >= count) break;
+            const int64_t t = idx[k];
+            const int64_t nt = n[t];
+            const int64_t ao = aoff[t], so = soff[t];
+            const int rc = nt <= 4 ? oracle_micro_solve(nt, A + ao, U + ao, S + so, Vt + ao, &info)
+                                   : oracle_small_solve(nt, A + ao, U + ao, S + so, Vt + ao, &info);
+            if (rc == 0) done.fetch_add(1);
+        }
+    };
+    const int nt = threads > 0 ? threads : 1;
+    std::vector<std::thread> pool;
+    pool.reserve(size_t(nt));
+    for (int i = 0; i < nt; ++i) pool.emplace_back(worker);
+    for (auto& th : pool) th.join();
+    return done.load();
 }
 
 }  // extern "C"

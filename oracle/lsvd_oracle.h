@@ -49,6 +49,14 @@ int oracle_small_solve_rectangular(int64_t m, int64_t d, const double* A, double
 /* qr_reduce (src/lie_svd_small.rs:373-418). A m*d (m>=d); Q m*d, R d*d. */
 int oracle_qr_reduce(int64_t m, int64_t d, const double* A, double* Q, double* R);
 
+/* Timed-baseline batch driver: matrices idx[0..count) of a packed uneven
+ * batch (matrix t: n[t] x n[t] at element offset aoff[t], singular values at
+ * soff[t]) on `threads` host threads, LieSvdMicro for n <= 4 and LieSvdSmall
+ * otherwise.  Returns the number solved. */
+int64_t oracle_svd_batch(int64_t count, const int32_t* idx, const int32_t* n, const int64_t* aoff,
+                         const int64_t* soff, const double* A, double* U, double* S, double* Vt,
+                         int32_t threads);
+
 /* LieSvdMicro::solve (src/lie_svd_micro.rs:21-52), n in 0..4. */
 int oracle_micro_solve(int64_t n, const double* A, double* U, double* S, double* Vt,
                        oracle_small_info* info);

@@ -64,6 +64,9 @@ def lib():
                                          C.POINTER(JointTrace)]
         _lib.oracle_joint_svd.argtypes = [C.c_int64, C.c_int64, C.c_int64, P, JointParams, P, P,
                                           P, C.POINTER(JointTrace)]
+        V = C.c_void_p
+        _lib.oracle_svd_batch.restype = C.c_int64
+        _lib.oracle_svd_batch.argtypes = [C.c_int64, V, V, V, V, V, V, V, V, C.c_int32]
     return _lib
 
 
@@ -73,6 +76,26 @@ def _p(a):
 
 def _c(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def svd_batch(ns, a, idx, threads: int, out=None):
+    """Solves matrices ``idx`` of the packed uneven batch ``(ns, a)`` on
+    ``threads`` host threads in one call (micro route for n <= 4, small
+    otherwise).  Returns ``(solved, U, S, Vt)`` in the packed layout."""
+    ns = np.ascontiguousarray(ns, dtype=np.int32)
+    a = _c(a)
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    aoff = np.zeros(ns.size + 1, dtype=np.int64)
+    aoff[1:] = np.cumsum(ns.astype(np.int64) ** 2)
+    soff = np.zeros(ns.size + 1, dtype=np.int64)
+    soff[1:] = np.cumsum(ns.astype(np.int64))
+    if out is None:
+        out = (np.empty_like(a), np.empty(int(soff[-1])), np.empty_like(a))
+    u, s, vt = out
+    v = lambda x: C.c_void_p(x.ctypes.data)  # noqa: E731
+    got = lib().oracle_svd_batch(idx.size, v(idx), v(ns), v(aoff), v(soff), v(a), v(u), v(s), v(vt),
+                                 int(threads))
+    return int(got), u, s, vt
 
 
 class LieSvdSmall:

@@ -75,3 +75,35 @@ def test_jade_trivial_sizes():
     mats = _family(3, 2, 5)
     v, diags, tr = LieSvdJoint.diagonalize_symmetric(mats)
     assert np.linalg.norm(v.T @ v - np.eye(3)) < 1e-12
+
+
+def test_jade_cfg4_size_vs_oracle():
+    # the benchmark's family shape (K = 64 symmetric 256 x 256 matrices,
+    # A_k = Q diag(d_k) Q^T + eps E_k) at all three eps, one family each,
+    # against the oracle: final off-diagonal, sorted diagonals, sweeps (within
+    # one) and rejected rotations
+    import concurrent.futures as cf
+    n, K = 256, 64
+    fams = {eps: P.jade_family_workload(1, K, n, eps, seed=4000 + i)
+            for i, eps in enumerate((0.0, 1e-8, 1e-4))}
+
+    def run_oracle(eps):
+        return eps, O.LieSvdJoint.diagonalize_symmetric([fams[eps][0, k] for k in range(K)])
+
+    with cf.ThreadPoolExecutor(3) as ex:
+        ores = dict(ex.map(run_oracle, fams))
+    for eps, fam in fams.items():
+        v, d, tr = LieSvdJoint.diagonalize_families(fam)
+        vo, do, tro = ores[eps]
+        scale = np.sqrt(np.sum(fam[0] ** 2))
+        assert np.linalg.norm(v[0].T @ v[0] - np.eye(n)) < 1e-10
+        assert abs(tr[0].initial_offdiag - tro.initial_offdiag) <= 1e-12 * tro.initial_offdiag
+        assert tr[0].final_offdiag <= max(10 * tro.final_offdiag, 1e-12 * scale), (eps, tr[0], tro)
+        assert abs(tr[0].sweeps - tro.sweeps) <= 1, (eps, tr[0].sweeps, tro.sweeps)
+        assert abs(tr[0].rejected_rotations - tro.rejected_rotations) <= max(2, tro.rejected_rotations // 10), \
+            (eps, tr[0].rejected_rotations, tro.rejected_rotations)
+        # the joint eigenvalues: equal to the oracle's up to the order of V's columns,
+        # within the off-diagonal mass both leave behind
+        tol = 1e-9 * scale + 2 * max(tr[0].final_offdiag, tro.final_offdiag)
+        for k in range(K):
+            assert np.max(np.abs(np.sort(d[0, k]) - np.sort(np.asarray(do[k])))) <= tol, (eps, k)

@@ -3,6 +3,8 @@ src/lie_svd_small.rs:158-183, on large m x n inputs) and its tcgen05 product
 kernel.
 
 Bars:
+* FP64 GEMM (mma.sync m8n8k4): against numpy's FP64 product, elementwise
+  |C - C_ref| <= 4 K eps (|A||B|) (both sum K products in FP64).
 * tcgen05 GEMM: against the FP64 product of the same TF32/BF16-rounded
   operands, |C - C_ref| <= K 2^-22 (|A||B|^T) elementwise (FP32 accumulation),
   relative Frobenius error <= 4 sqrt(K) 2^-24.
@@ -21,7 +23,7 @@ import pytest
 import oracle as O
 from lie_cliffalg_analog_svd_b200 import LsvdError, polar
 from lie_cliffalg_analog_svd_b200 import profiles as P
-from lie_cliffalg_analog_svd_b200.api import gemm_nt_lowp
+from lie_cliffalg_analog_svd_b200.api import gemm_f64, gemm_nt_lowp
 
 pytestmark = pytest.mark.gpu
 
@@ -38,6 +40,30 @@ def _round_tf32(x: np.ndarray) -> np.ndarray:
 def _round_bf16(x: np.ndarray) -> np.ndarray:
     import torch
     return torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).to(torch.bfloat16).float().numpy()
+
+
+@pytest.mark.parametrize("ta,tb", [(False, False), (True, False), (False, True), (True, True)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 16), (1, 1, 1), (7, 9, 5), (130, 257, 33), (300, 200, 1000),
+                                   (512, 384, 4096), (64, 1000, 3)])
+def test_gemm_f64(ta, tb, M, N, K):
+    import torch
+    rng = np.random.default_rng(M * 13 + N * 5 + K + 2 * ta + tb)
+    a = rng.standard_normal((K, M) if ta else (M, K))
+    b = rng.standard_normal((N, K) if tb else (K, N))
+    c0 = rng.standard_normal((M, N))
+    pad = lambda x: np.pad(x, ((0, 0), (0, (-x.shape[1]) % 2)))  # noqa: E731  (even row stride)
+    ad = torch.from_numpy(pad(a)).cuda()[:, :a.shape[1]]
+    bd = torch.from_numpy(pad(b)).cuda()[:, :b.shape[1]]
+    cd = torch.from_numpy(c0.copy()).cuda()
+    gemm_f64(ad, bd, ta, tb, alpha=1.5, beta=-0.5, c=cd)
+    opa, opb = (a.T if ta else a), (b.T if tb else b)
+    ref = 1.5 * (opa @ opb) - 0.5 * c0
+    mag = 1.5 * (np.abs(opa) @ np.abs(opb)) + 0.5 * np.abs(c0)
+    assert np.all(np.abs(cd.cpu().numpy() - ref) <= 4 * max(K, 1) * 2.2e-16 * mag + 1e-300)
+    # beta = 0 must not read C (NaN in C stays out of the result)
+    cn = torch.full((M, N), float("nan"), dtype=torch.float64, device="cuda")
+    gemm_f64(ad, bd, ta, tb, c=cn)
+    assert torch.isfinite(cn).all()
 
 
 @pytest.mark.parametrize("prec", ["tf32", "bf16"])

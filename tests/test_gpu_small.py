@@ -371,3 +371,57 @@ def test_batched_host_pipeline_matches_device():
     # pageable host memory takes the same path (its copies are then synchronous)
     u2, s2, vt2, _, st2 = svd_batched(ns, a)
     assert st2 == 0 and np.array_equal(s2, s)
+
+
+def test_batched_host_pipeline_uniform_n_matches_device():
+    # a uniform size list gives chunks with equal size lists: each chunk must
+    # still stage through its own buffers (results bit-identical to the
+    # device-pointer call)
+    import torch
+    count, n = 16384, 16
+    ns = np.full(count, n, dtype=np.int32)
+    a = np.random.default_rng(123).standard_normal(count * n * n)
+    pin = lambda k: torch.empty(k, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    a_h = pin(a.size)
+    a_h[:] = a
+    out_h = (pin(a.size), pin(count * n), pin(a.size), None)
+    u, s, vt, _, st = svd_batched(ns, a_h, out=out_h)
+    assert st == 0
+    ud, sd, vtd, _, std = svd_batched(ns, torch.from_numpy(a).cuda())
+    assert std == 0
+    assert np.array_equal(s, sd.cpu().numpy())
+    assert np.array_equal(u, ud.cpu().numpy()) and np.array_equal(vt, vtd.cpu().numpy())
+    # a second call reuses the per-chunk plans and must give the same bits
+    u2, s2, vt2, _, st2 = svd_batched(ns, a_h, out=(pin(a.size), pin(count * n), pin(a.size), None))
+    assert st2 == 0 and np.array_equal(s2, s) and np.array_equal(u2, u)
+
+
+def test_batched_timed_mode_matches_oracle():
+    # the benchmark's mode (no LSVD_WANT_DIAG): U, S and Vt of >= 1000
+    # matrices across n = 2..64 with the kappa <= 1e12 / degenerate mix,
+    # checked against the oracle matrix by matrix
+    import concurrent.futures as cf
+    ns, a, sig = P.uneven_batch_workload(1200, seed=2024)
+    u, s, vt, _, st = svd_batched(ns, a)
+    assert st == L.OK
+    us, ss, vts, as_ = unpack(ns, u), unpack(ns, s, square=False), unpack(ns, vt), unpack(ns, a)
+
+    def one(t):
+        n = int(ns[t])
+        uo, so, vo = O.LieSvdMicro.solve(as_[t]) if n <= 4 else O.LieSvdSmall.solve(as_[t])
+        return t, uo, so, vo
+
+    with cf.ThreadPoolExecutor(8) as ex:
+        res = list(ex.map(one, range(len(ns))))
+    for t, uo, so, vo in res:
+        n = int(ns[t])
+        assert sigma_err(ss[t], so) < 1e-13, (t, n)
+        r, ou, ov = mets(as_[t], us[t], ss[t], vts[t])
+        ro, ouo, ovo = mets(as_[t], uo, so, vo)
+        assert r < max(4e-13, 8 * ro) and ou < max(2e-13, 8 * ouo) and ov < max(2e-13, 8 * ovo), (t, n)
+        # separated singular directions agree with the oracle's up to sign
+        for j in range(n):
+            gap = min([abs(so[j] - so[k]) for k in (j - 1, j + 1) if 0 <= k < n] + [np.inf])
+            if so[j] > 1e-6 * so[0] and gap > 1e-6 * so[0]:
+                assert abs(us[t][:, j] @ uo[:, j]) >= 1 - 1e-9, (t, n, j)
+                assert abs(vts[t][j] @ vo[j]) >= 1 - 1e-9, (t, n, j)

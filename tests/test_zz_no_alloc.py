@@ -1,6 +1,5 @@
 """lsvd_svd_batched_noalloc_f64: the batched FP64 SVD for callers that cannot
-allocate device memory (code running under CUDA-graph stream capture, where
-cudaMalloc is not allowed; latency-critical loops that cannot take the
+allocate device memory (latency-critical loops that cannot take the
 device-wide synchronisation of cudaMalloc/cudaFree; hosts whose device memory
 belongs to their own allocator).  The entry point keeps its working memory in
 a static device array; this test hands it preallocated device buffers through
@@ -34,14 +33,20 @@ def _noalloc(lib, stream, ns, a_dev, u, s, vt, dg):
         C.c_void_p(dg.data_ptr()), L.WANT_DIAG)
 
 
-def test_noalloc_matches_batched_twice():
+def test_noalloc_matches_batched_twice(monkeypatch, tmp_path):
     import torch
+    from lie_cliffalg_analog_svd_b200 import Context
+    # both entry points on the built-in team shapes: no LSVD_SHAPES override,
+    # no autotune cache, a fresh context (no plan cached under other shapes)
+    monkeypatch.delenv("LSVD_SHAPES", raising=False)
+    monkeypatch.setenv("LSVD_AUTOTUNE_CACHE", str(tmp_path / "none.json"))
+    ctx = Context(0)
     lib = L.load()
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream(dev).cuda_stream
     for seed, count in ((31, 3000), (32, 1200)):
         ns, a, _ = P.uneven_batch_workload(count, seed=seed)
-        ref_u, ref_s, ref_vt, ref_dg, st = svd_batched(ns, a, want_diag=True)
+        ref_u, ref_s, ref_vt, ref_dg, st = svd_batched(ns, a, want_diag=True, ctx=ctx)
         assert st == L.OK
         ad = torch.from_numpy(a).to(dev)
         u = torch.empty_like(ad)
@@ -57,6 +62,7 @@ def test_noalloc_matches_batched_twice():
         d = np.frombuffer(dg.cpu().numpy().tobytes(), dtype=L.DIAG_DTYPE)
         assert np.all(d["orth_u"] < 4e-13) and np.all(d["rel_recon"] < 4e-13)
         assert np.array_equal(d["route"], ref_dg["route"])
+    ctx.close()
 
 
 def test_noalloc_rejects_too_many_matrices():
