@@ -117,6 +117,7 @@ lsvd_context::~lsvd_context() {
         b->release();
     if (pinned) cudaFreeHost(pinned);
     if (h2d_stream) cudaStreamDestroy(h2d_stream);
+    if (side_stream) cudaStreamDestroy(side_stream);
     if (d2h_stream) cudaStreamDestroy(d2h_stream);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }

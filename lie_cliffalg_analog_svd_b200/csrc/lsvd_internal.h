@@ -89,6 +89,8 @@ struct lsvd_context {
     DeviceBuffer ws_large;  // large SVD: A, the [G; V] panel store, Gram partials, rotations
     // copy streams of the pipelined host-pointer batched path, created on first use
     cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
+    // side branch of the large solve's sweep graph (V's update), created on first use
+    cudaStream_t side_stream = nullptr;
     std::unordered_map<uint64_t, std::unique_ptr<BatchPlan>> plans;
     // one plan per chunk of the pipelined host-pointer path: every chunk owns
     // its staging buffers, even when two chunks have the same size list

@@ -914,26 +914,57 @@ static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, 
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     char* p = ws;
     SweepState* stt = reinterpret_cast<SweepState*>(p); p += al(sizeof(SweepState));
-    int* skip = reinterpret_cast<int*>(p); p += al(size_t(npairs) * 4);
-    double* Rg = reinterpret_cast<double*>(p);
+    // rotations and skip flags double-buffered by layer parity: V's update of
+    // layer L runs on a side branch of the graph while the next layer solves
+    int* skip2[2];
+    double* Rg2[2];
+    skip2[0] = reinterpret_cast<int*>(p); p += al(size_t(npairs) * 4);
+    skip2[1] = reinterpret_cast<int*>(p); p += al(size_t(npairs) * 4);
+    Rg2[0] = reinterpret_cast<double*>(p); p += al(size_t(npairs) * PW * PW * 8);
+    Rg2[1] = reinterpret_cast<double*>(p);
     cudaError_t e = cudaMemsetAsync(stt, 0, sizeof(SweepState), st);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(solve2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(twoside_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTwoSmem);
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: sweep setup");
+    if (!ctx->side_stream && (e = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: side stream");
+    cudaStream_t sv = ctx->side_stream;
+    cudaEvent_t evs[4] = {nullptr, nullptr, nullptr, nullptr};  // fork, join, applied[2]
+    for (auto& x : evs)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+    auto destroy_events = [&]() {
+        for (auto& x : evs)
+            if (x) cudaEventDestroy(x);
+    };
+    if (e != cudaSuccess) {
+        destroy_events();
+        return lsvd_ctx_cuda(ctx, e, "large: capture events");
+    }
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+        destroy_events();
         return lsvd_ctx_cuda(ctx, e, "large: begin capture");
+    }
     offnorm_kernel<<<1, 1024, 0, st>>>(P, npad, n, stt, limit);
     for (int layer = 0; layer < nb - 1; ++layer) {
-        solve2_kernel<<<npairs, 256, kSolveSmem, st>>>(P, npad, nb, layer, Rg, skip, stt, tau, inner_max);
-        twoside_kernel<<<ntri, 256, kTwoSmem, st>>>(P, npad, nb, layer, Rg, skip, stt);
-        apply_kernel<<<dim3(npairs, napply), 256, kApplySmem, st>>>(Vc, npad, nb, layer, rows, Rg, skip, stt);
+        const int b = layer & 1;
+        // the buffers of parity b were last read by V's update two layers back
+        if (layer >= 2) cudaStreamWaitEvent(st, evs[2 + b], 0);
+        solve2_kernel<<<npairs, 256, kSolveSmem, st>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt, tau, inner_max);
+        cudaEventRecord(evs[0], st);
+        cudaStreamWaitEvent(sv, evs[0], 0);
+        apply_kernel<<<dim3(npairs, napply), 256, kApplySmem, sv>>>(Vc, npad, nb, layer, rows, Rg2[b], skip2[b], stt);
+        cudaEventRecord(evs[2 + b], sv);
+        twoside_kernel<<<ntri, 256, kTwoSmem, st>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt);
     }
+    cudaEventRecord(evs[1], sv);
+    cudaStreamWaitEvent(st, evs[1], 0);
     sweep_end_kernel<<<1, 1, 0, st>>>(stt, -1.0);
     cudaError_t e2 = cudaGetLastError();
     e = cudaStreamEndCapture(st, &graph);
+    destroy_events();
     if (e2 != cudaSuccess || e != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         return lsvd_ctx_cuda(ctx, e2 != cudaSuccess ? e2 : e, "large: sweep capture");
@@ -996,7 +1027,9 @@ static size_t sweep_ws_bytes(int gpad, int npad, int num_sms) {
     const int nb = npad / BW, npairs = nb / 2;
     const int nchunk = std::max(1, std::min(gpad / 64, (3 * num_sms + npairs - 1) / npairs));
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    return al(sizeof(SweepState)) + al(size_t(npairs) * 4) + al(size_t(npairs) * PW * PW * 8) +
+    // state | skip x 2 | rotations x 2 | Gram partials (the two-sided route uses the second
+    // skip and rotation buffers, the one-sided route the partials)
+    return al(sizeof(SweepState)) + 2 * al(size_t(npairs) * 4) + 2 * al(size_t(npairs) * PW * PW * 8) +
            al(size_t(npairs) * (nchunk + 1) * PW * PW * 8);
 }
 
@@ -1101,7 +1134,9 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
         //    rounding level eps ||P||_F / sqrt(n) of the entries
         const double refn = std::max(std::sqrt(p2), 1e-300);
         const double tau = 2.220446049250313e-16 * refn / std::sqrt(double(npad));
-        jst = run_sweeps2(ctx, P2, Vc, int(n), npad, 1e-13 * refn, tau, 40, 8, sw, &sweeps, &rots, &off,
+        // one inner Jacobi sweep per block solve: a full diagonalisation of
+        // every 64 x 64 block saves about one outer sweep but costs eight
+        jst = run_sweeps2(ctx, P2, Vc, int(n), npad, 1e-13 * refn, tau, 40, 1, sw, &sweeps, &rots, &off,
                           &inner_cap, &ms_eig);
         if (jst != LSVD_OK && jst != LSVD_NOT_CONVERGED) return jst;
         if (jst == LSVD_NOT_CONVERGED) mflags |= LSVD_MAT_JACOBI_CAP;
