@@ -169,12 +169,22 @@ typedef struct lsvd_large_info {
  * LieSvdSmall::solve, src/lie_svd_small.rs:296-323, and solve_rectangular,
  * :340-360, run at any size; the reference routes up to n = 512 there,
  * src/lie_svd_adaptive.rs:71).  A m x n (lda); k = min(m, n); U m x k (ldu),
- * S k (descending), Vt k x n (ldvt).  FP64: Newton-Schulz polar factor Q of
- * A (or of A^T when n > m) on the FP64 tensor path, P = sym(Q^T A), V and
- * sigma = max(lambda, 0) by blocked one-sided Jacobi on P (blocks of 32
- * columns, 64 x 64 block-pair rotations applied as FP64 tensor products,
- * convergence flag on the device), U = Q V.  Host or device pointers
- * (LSVD_DEVICE_POINTERS); synchronous.  `info` may be NULL. */
+ * S k (descending), Vt k x n (ldvt).
+ *   LSVD_PREC_FP64: Newton-Schulz polar factor Q of A (or of A^T when n > m)
+ *     on the FP64 tensor path, P = sym(Q^T A), V by blocked two-sided Jacobi
+ *     on P (blocks of 32 indices, 64 x 64 block-pair rotations applied as
+ *     FP64 tensor products, the reference's stop test off(P) < 1e-13 ||P||_F
+ *     evaluated on the device), sigma = max(lambda, 0) from the Rayleigh
+ *     quotients, U = Q V.
+ *   LSVD_PREC_MIXED_TF32/BF16 (m, n multiples of 128): the Newton-Schulz
+ *     bulk on the tcgen05 tensor cores gives Q0; the eigensolve of
+ *     P0 = sym(Q0^T A) stops at the low-precision level (4 u ||P0||_F) and
+ *     gives V0; FP64 blocked one-sided Jacobi on W = A V0 then orthogonalises
+ *     the columns (accuracy comes from this FP64 stage on A itself):
+ *     sigma_j = ||w_j||, U = W diag(sigma)^-1, V = V0 R.  A zero singular
+ *     value leaves its U column zero (LSVD_MAT_REPAIRED set in info.flags).
+ * Host or device pointers (LSVD_DEVICE_POINTERS); synchronous.  `info` may
+ * be NULL. */
 LSVD_API lsvd_status lsvd_svd_large_f64(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,
                                         double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
                                         lsvd_precision precision, lsvd_large_info* info, uint32_t flags);

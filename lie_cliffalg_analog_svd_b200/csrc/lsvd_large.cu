@@ -681,6 +681,27 @@ __global__ void gather_vt_kernel(const double* H, int64_t ldh, int gpad, int n, 
     }
 }
 
+// U (m x k, ldu) column k = g_{perm[k]} / sigma_k from the one-sided panel
+// store (H row j = column j of G), transposed through 32 x 32 shared tiles.
+__global__ void gather_u_kernel(const double* H, int64_t ldh, int m, int k, const int* perm, const double* inv,
+                                double* U, int64_t ldu) {
+    __shared__ double tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    for (int k0 = blockIdx.y * 32; k0 < k; k0 += gridDim.y * 32)
+        for (int i0 = blockIdx.x * 32; i0 < m; i0 += gridDim.x * 32) {
+            for (int r = ty; r < 32; r += 8) {
+                const int kk = k0 + r, i = i0 + tx;
+                tile[r][tx] = (kk < k && i < m) ? H[int64_t(perm[kk]) * ldh + i] * inv[kk] : 0.0;
+            }
+            __syncthreads();
+            for (int r = ty; r < 32; r += 8) {
+                const int i = i0 + r, kk = k0 + tx;
+                if (i < m && kk < k) U[int64_t(i) * ldu + kk] = tile[tx][r];
+            }
+            __syncthreads();
+        }
+}
+
 __global__ void frob2_part_kernel(int m, int n, const double* A, int64_t lda, double* part) {
     __shared__ double red[256];
     double s = 0.0;
@@ -1045,9 +1066,14 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t b_a = al(size_t(m) * ld * 8), b_p = al(size_t(ld) * ld * 8), b_h = al(size_t(npad) * ldh * 8);
     const size_t b_u = al(size_t(m) * ld * 8), b_v = al(size_t(ld) * ld * 8);
-    const size_t b_misc = al(4096 * 8 + 64) + al(size_t(n) * 8) + al(size_t(n) * 4);
-    const size_t b_sw = sweep_ws_bytes(gpad, npad, ctx->num_sms);
-    char* ws = static_cast<char*>(ctx->ws_large.get(b_a + b_p + b_h + b_u + b_v + b_misc + b_sw, &e));
+    const size_t b_misc = al(4096 * 8 + 64) + al(size_t(n) * 8) * 2 + al(size_t(n) * 4);
+    const bool lowp = precision == LSVD_PREC_MIXED_TF32 || precision == LSVD_PREC_MIXED_BF16;
+    // mixed route: the one-sided panel store [W; V] with W = A V0 (m rows)
+    const int gpadm = int((m + 63) & ~int64_t(63));
+    const int64_t ldh1 = int64_t(gpadm) + npad;
+    const size_t b_h1 = lowp ? al(size_t(npad) * ldh1 * 8) : 0;
+    const size_t b_sw = sweep_ws_bytes(std::max(gpad, lowp ? gpadm : 0), npad, ctx->num_sms);
+    char* ws = static_cast<char*>(ctx->ws_large.get(b_a + b_p + b_h + b_u + b_v + b_misc + b_h1 + b_sw, &e));
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: workspace");
     char* p = ws;
     double* A64 = reinterpret_cast<double*>(p); p += b_a;
@@ -1059,7 +1085,10 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
     double* dsum = part + 4096;
     p += al(4096 * 8 + 64);
     double* sig = reinterpret_cast<double*>(p); p += al(size_t(n) * 8);
+    double* sig2 = reinterpret_cast<double*>(p); p += al(size_t(n) * 8);
     int* perm_d = reinterpret_cast<int*>(p); p += al(size_t(n) * 4);
+    double* H1 = lowp ? reinterpret_cast<double*>(p) : nullptr;
+    p += b_h1;
     char* sw = p;
     // A (m x n) into A64 with an even leading dimension (transposed input: A is n x m)
     if ((e = cudaMemsetAsync(A64, 0, size_t(m) * ld * 8, st)) != cudaSuccess)
@@ -1098,14 +1127,22 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
     tpol.start(st);
     lsvd_status pst = LSVD_OK;
     if (f2 > 0.0) {
-        pst = lsvd_polar_run(ctx, m, n, A64, ld, LSVD_PREC_FP64, 120, &X, &ldx, &pinfo);
+        // FP64: the reference's iteration to delta < 1e-13 sqrt(n).  Mixed: the
+        // TF32/BF16 tensor-core bulk only (no FP64 iterations): its factor Q0
+        // preconditions the eigensolve below and accuracy comes from the FP64
+        // cleanup on A itself.
+        pst = lsvd_polar_run(ctx, m, n, A64, ld, lowp ? precision : LSVD_PREC_FP64, lowp ? 0 : 120, &X, &ldx,
+                             &pinfo);
         if (pst != LSVD_OK && pst != LSVD_NOT_CONVERGED) return pst;
+        if (lowp) pst = LSVD_OK;
     }
     tpol.stop(st);
     if (pst == LSVD_NOT_CONVERGED) mflags |= LSVD_MAT_NS_CAP;
-    if (f2 > 0.0 && pinfo.orth > 1e-8 * std::sqrt(double(n))) mflags |= LSVD_MAT_POLAR_UNTRUSTED;
+    if (!lowp && f2 > 0.0 && pinfo.orth > 1e-8 * std::sqrt(double(n))) mflags |= LSVD_MAT_POLAR_UNTRUSTED;
     li.ns_iters_fp64 = pinfo.iters_fp64;
+    li.ns_iters_lowp = pinfo.iters_lowp;
     li.flops_fp64 += pinfo.flops_fp64;
+    li.flops_lowp += pinfo.flops_lowp;
     // scale G so that ||P||_F = ||A||_F is near 1 (a power of two: exact)
     const double scale = f2 > 0.0 ? std::ldexp(1.0, -std::ilogb(std::sqrt(f2))) : 1.0;
     int sweeps = 0, inner_cap = 0;
@@ -1134,9 +1171,12 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
         //    rounding level eps ||P||_F / sqrt(n) of the entries
         const double refn = std::max(std::sqrt(p2), 1e-300);
         const double tau = 2.220446049250313e-16 * refn / std::sqrt(double(npad));
+        // mixed: P0 = Q0^T A is accurate to ~u_lo ||A|| only, so its eigensolve
+        // stops at off(P0) < 4 u_lo ||P0||_F (TF32 u = 2^-11, BF16 2^-8)
+        const double stop = lowp ? 4.0 * (precision == LSVD_PREC_MIXED_BF16 ? 3.90625e-3 : 4.8828125e-4) : 1e-13;
         // one inner Jacobi sweep per block solve: a full diagonalisation of
         // every 64 x 64 block saves about one outer sweep but costs eight
-        jst = run_sweeps2(ctx, P2, Vc, int(n), npad, 1e-13 * refn, tau, 40, 1, sw, &sweeps, &rots, &off,
+        jst = run_sweeps2(ctx, P2, Vc, int(n), npad, stop * refn, tau, 40, 1, sw, &sweeps, &rots, &off,
                           &inner_cap, &ms_eig);
         if (jst != LSVD_OK && jst != LSVD_NOT_CONVERGED) return jst;
         if (jst == LSVD_NOT_CONVERGED) mflags |= LSVD_MAT_JACOBI_CAP;
@@ -1145,13 +1185,57 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
         const double np2 = double(npad / PW);
         li.flops_fp64 += double(sweeps) * double(npad / BW - 1) *
                          (np2 * (np2 + 1) / 2 * 4.0 * PW * PW * PW + np2 * 2.0 * PW * PW * npad);
-        // 4. eigenvalues: Rayleigh quotients of the original P for the converged basis
-        if ((e = lsvd::dg::dgemm(st, false, true, int(n), int(n), int(n), 1.0, Vc, npad, Pm, ld, 0.0, Ud, ld)) !=
-            cudaSuccess)
-            return lsvd_ctx_cuda(ctx, e, "large: P V");
-        li.flops_fp64 += 2.0 * double(n) * double(n) * double(n);
-        rayleigh_kernel<<<(int(n) * 32 + 255) / 256, 256, 0, st>>>(Vc, npad, Ud, ld, int(n), sig);
-        ctx->launches += 2;
+        if (!lowp) {
+            // 4. eigenvalues: Rayleigh quotients of the original P for the converged basis
+            if ((e = lsvd::dg::dgemm(st, false, true, int(n), int(n), int(n), 1.0, Vc, npad, Pm, ld, 0.0, Ud,
+                                     ld)) != cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: P V");
+            li.flops_fp64 += 2.0 * double(n) * double(n) * double(n);
+            rayleigh_kernel<<<(int(n) * 32 + 255) / 256, 256, 0, st>>>(Vc, npad, Ud, ld, int(n), sig);
+            ctx->launches += 2;
+        } else {
+            // 4'. FP64 cleanup on A itself: W = A V0, then blocked one-sided Jacobi on
+            //     the panel store [W; V0] until the columns of W are orthogonal (the
+            //     normwise-scaled test of solve_kernel); sigma_j = ||w_j||, U = W / sigma
+            li.sweeps_lowp = sweeps;
+            li.ms_eig_lowp = ms_eig;
+            if ((e = lsvd::dg::dgemm(st, false, true, int(m), int(n), int(n), 1.0, A64, ld, Vc, npad, 0.0, Ud,
+                                     ld)) != cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: W = A V0");
+            li.flops_fp64 += 2.0 * double(m) * double(n) * double(n);
+            if ((e = cudaMemsetAsync(H1, 0, size_t(npad) * ldh1 * 8, st)) != cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: clear H");
+            transpose_kernel<<<dim3(64, 32), 256, 0, st>>>(int(m), int(n), Ud, ld, H1, ldh1);
+            if ((e = cudaMemcpy2DAsync(H1 + gpadm, size_t(ldh1) * 8, Vc, size_t(npad) * 8, size_t(npad) * 8,
+                                       size_t(npad), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: V0 into H");
+            colnorm_kernel<<<(int(n) * 32 + 255) / 256, 256, 0, st>>>(H1, ldh1, int(n), int(m), gpadm, 0, sig);
+            ctx->launches += 3;
+            std::vector<double> c0(static_cast<size_t>(n));
+            if ((e = cudaMemcpyAsync(c0.data(), sig, size_t(n) * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(st)) != cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: column norms");
+            double s2 = 0.0;
+            for (double v : c0) s2 = std::max(s2, v * v);
+            const double tol1 = std::max(1e-14, 8.0 * 2.220446049250313e-16 * std::sqrt(double(gpadm)));
+            int sw1 = 0, cap1 = 0;
+            int64_t rot1 = 0;
+            double off1 = 0.0, ms1 = 0.0;
+            jst = run_sweeps(ctx, H1, ldh1, int(m), gpadm, npad, tol1, 1e-10, s2, 40, 2, sw, &sw1, &rot1, &off1,
+                             &cap1, &ms1);
+            if (jst != LSVD_OK && jst != LSVD_NOT_CONVERGED) return jst;
+            if (jst == LSVD_NOT_CONVERGED) mflags |= LSVD_MAT_JACOBI_CAP;
+            sweeps = sw1;
+            rots += rot1;
+            off = off1;
+            inner_cap += cap1;
+            ms_eig = ms1;
+            // per sweep and layer: Gram over gpadm rows and the apply over ldh1 rows, per block pair
+            li.flops_fp64 += double(sw1) * double(npad / BW - 1) * double(npad / PW) * 2.0 * PW * PW *
+                             double(gpadm + ldh1);
+            colnorm_kernel<<<(int(n) * 32 + 255) / 256, 256, 0, st>>>(H1, ldh1, int(n), int(m), gpadm, 0, sig);
+            ctx->launches += 1;
+        }
     } else {
         // A = 0: sigma = 0, V = I, U = the first n columns of I (MGS fill of zero seeds)
         fill_p2v_kernel<<<2048, 256, 0, st>>>(Pm, ld, 0, 0.0, P2, Vc, npad);
@@ -1171,13 +1255,28 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
     for (int64_t k = 0; k < n; ++k) hsorted[size_t(k)] = std::max(hs[size_t(perm[size_t(k)])], 0.0);
     if ((e = cudaMemcpyAsync(perm_d, perm.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return lsvd_ctx_cuda(ctx, e, "large: perm");
-    gather_vt_kernel<<<2048, 256, 0, st>>>(Vc, npad, 0, int(n), perm_d, Vd, ld);
-    if (f2 > 0.0) {
+    if (lowp && f2 > 0.0) {
+        // U = W / sigma and Vt from the one-sided panel store
+        std::vector<double> inv(static_cast<size_t>(n));
+        for (int64_t k = 0; k < n; ++k) {
+            inv[size_t(k)] = hsorted[size_t(k)] > 0.0 ? 1.0 / hsorted[size_t(k)] : 0.0;
+            if (!(hsorted[size_t(k)] > 0.0)) mflags |= LSVD_MAT_REPAIRED;  // zero column left zero
+        }
+        if ((e = cudaMemcpyAsync(sig2, inv.data(), size_t(n) * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+            return lsvd_ctx_cuda(ctx, e, "large: 1/sigma");
+        gather_vt_kernel<<<2048, 256, 0, st>>>(H1, ldh1, gpadm, int(n), perm_d, Vd, ld);
+        gather_u_kernel<<<dim3(64, 32), 256, 0, st>>>(H1, ldh1, int(m), int(n), perm_d, sig2, Ud, ld);
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess)  // `inv` is pageable host memory
+            return lsvd_ctx_cuda(ctx, e, "large: gather");
+    } else {
+        gather_vt_kernel<<<2048, 256, 0, st>>>(Vc, npad, 0, int(n), perm_d, Vd, ld);
+    }
+    if (f2 > 0.0 && !lowp) {
         if ((e = lsvd::dg::dgemm(st, false, true, int(m), int(n), int(n), 1.0, X, ldx, Vd, ld, 0.0, Ud, ld)) !=
             cudaSuccess)
             return lsvd_ctx_cuda(ctx, e, "large: U = Q V");
         li.flops_fp64 += 2.0 * double(m) * double(n) * double(n);
-    } else {
+    } else if (f2 == 0.0) {
         std::vector<double> eye(size_t(m) * ld, 0.0);
         for (int64_t i = 0; i < n; ++i) eye[size_t(i) * ld + i] = 1.0;
         if ((e = cudaMemcpyAsync(Ud, eye.data(), eye.size() * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
@@ -1258,7 +1357,7 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
     if ((e = cudaMemcpyAsync(S, hsorted.data(), size_t(n) * 8, cudaMemcpyDefault, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return lsvd_ctx_cuda(ctx, e, "large: copy S");
-    li.sweeps_fp64 = sweeps;
+    li.sweeps_fp64 = sweeps;  // mixed: the FP64 cleanup sweeps
     li.rotations = rots;
     li.flags = mflags;
     li.last_offdiag = off;
@@ -1272,7 +1371,6 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
         li.orth_v = diag->orth_v;
     }
     if (info) *info = li;
-    (void)precision;
     if (jst == LSVD_NOT_CONVERGED || pst == LSVD_NOT_CONVERGED) return LSVD_NOT_CONVERGED;
     return LSVD_OK;
 }
@@ -1296,8 +1394,10 @@ extern "C" lsvd_status lsvd_svd_large_f64(lsvd_context* ctx, int64_t m, int64_t 
         return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_svd_large_f64: bad pointer or leading dimension");
     if (std::max(m, n) > (int64_t(1) << 16) || k > 16384)
         return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "lsvd_svd_large_f64: larger than 65536 x 16384");
-    if (precision != LSVD_PREC_FP64)
-        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "lsvd_svd_large_f64: precision");
+    if (precision != LSVD_PREC_FP64 && precision != LSVD_PREC_MIXED_TF32 && precision != LSVD_PREC_MIXED_BF16)
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_svd_large_f64: unknown precision");
+    if (precision != LSVD_PREC_FP64 && (std::max(m, n) % 128 || std::min(m, n) % 128))
+        return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "lsvd_svd_large_f64: TF32/BF16 need m, n multiples of 128");
     cudaSetDevice(ctx->device);
     lsvd_diag d;
     return lsvd_large_solve(ctx, m, n, A, lda, U, ldu, S, Vt, ldvt, precision, info, &d,

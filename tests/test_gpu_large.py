@@ -145,3 +145,32 @@ def test_large_edge_cases():
     with pytest.raises(L.LsvdError) as ei:
         svd_large(bad)
     assert ei.value.status == L.NONFINITE_INPUT
+
+
+@pytest.mark.parametrize("prec", ["tf32", "bf16"])
+def test_mixed_route_matches_fp64_and_oracle(prec):
+    # TF32/BF16 tensor-core Newton-Schulz bulk, a preconditioning eigensolve to
+    # the low-precision level, then FP64 one-sided Jacobi on A V0: the same
+    # bars as the FP64 route (sigma 1e-13 normwise against the imposed
+    # spectrum, orthogonality and reconstruction), at kappa 1e2 / 1e5 / 1e8,
+    # square and tall, and the oracle at n = 512
+    for (m, n), kappa, seed in (((512, 512), 1e2, 11), ((640, 384), 1e5, 12), ((512, 512), 1e8, 13)):
+        q1, s, q2 = P.conditioned_factors(m, n, kappa, seed)
+        a = (q1 * s) @ q2.T
+        r = svd_large(a, prec)
+        assert r.status == L.OK, r.status
+        assert r.info.ns_iters_lowp > 0 and r.info.ns_iters_fp64 == 0 and r.info.sweeps_fp64 >= 1
+        assert sigma_err(r.s, s) <= 1e-13, (prec, kappa, sigma_err(r.s, s))
+        f = svd_large(a, "fp64")
+        assert sigma_err(r.s, f.s) <= 1e-13
+        floor = 2e-13 * max(1.0, n / 64)
+        rec, ou, ov = mets(a, r.u, r.s, r.vt)
+        assert rec <= floor and ou <= floor and ov <= floor, (prec, kappa, rec, ou, ov)
+        if (m, n) == (512, 512) and kappa == 1e2:
+            compare(a, (r.u, r.s, r.vt), O.LieSvdSmall.solve(a))
+
+
+def test_mixed_route_rejects_unaligned():
+    with pytest.raises(L.LsvdError) as ei:
+        svd_large(np.random.default_rng(0).standard_normal((300, 200)), "tf32")
+    assert ei.value.status == L.UNSUPPORTED
