@@ -203,6 +203,24 @@ LSVD_API lsvd_status lsvd_svd_batched_f64(lsvd_context* ctx, int64_t count, cons
                                           lsvd_diag* diags, lsvd_precision precision,
                                           uint32_t flags);
 
+/* Autotuner of the batched FP64 kernel (no counterpart in the reference):
+ * for every size class (n = 5..8, 9..16, 17..24, 25..32, 33..48, 49..64)
+ * times each feasible team shape (warps per team, GEMM register tile, lanes
+ * per Jacobi pair, matrices per team) on a seeded batch of `per_class`
+ * matrices (16..100000) with CUDA events on the context's stream, and writes
+ * the fastest to the shape cache (`cache_path`, or NULL for
+ * LSVD_AUTOTUNE_CACHE / $HOME/.cache/lsvd_b200/shapes.json) that the batched
+ * planner reads; the context's cached plans are dropped.  `report` (may be
+ * NULL) receives one line per class with the chosen and the default shape
+ * and their times.  Synchronous. */
+LSVD_API lsvd_status lsvd_autotune_f64(lsvd_context* ctx, int64_t per_class, const char* cache_path,
+                                       char* report, int64_t report_cap);
+/* The team shapes the batched planner uses now for `precision`
+ * (LSVD_SHAPES, then the autotune cache, then the built-in defaults):
+ * out[4c .. 4c+3] = warps per team, register tile, lanes per Jacobi pair,
+ * matrices per team for size class c = 0..7 (out holds 32 int32). */
+LSVD_API lsvd_status lsvd_class_shapes(lsvd_context* ctx, lsvd_precision precision, int32_t* out);
+
 /* No counterpart in the reference.  The batched FP64 SVD of
  * lsvd_svd_batched_f64 for callers that cannot allocate device memory:
  * latency-critical loops that cannot absorb the device-wide synchronisation

@@ -91,6 +91,8 @@ SIGNATURES = {
                                                    U32]),
     "lsvd_svd_batched_f64": (C.c_int, [P, I64, P, P, P, P, P, P, C.c_int, U32]),
     "lsvd_svd_large_f64": (C.c_int, [P, I64, I64, P, I64, P, I64, P, P, I64, C.c_int, P, U32]),
+    "lsvd_autotune_f64": (C.c_int, [P, I64, C.c_char_p, P, I64]),
+    "lsvd_class_shapes": (C.c_int, [P, C.c_int, P]),
     "lsvd_metrics_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, P, U32]),
     "lsvd_svd_batched_noalloc_f64": (C.c_int, [P, I64, P, P, P, P, P, P, U32]),
     "lsvd_joint_params_for_n": (JointParams, [I64]),

@@ -334,6 +334,28 @@ def svd_batched(ns, a, precision: str = "fp64", want_diag: bool = False,
     return u, s, vt, dg, st
 
 
+def autotune(per_class: int = 2000, cache_path: str | None = None, ctx: Context | None = None) -> str:
+    """Times the batched FP64 kernel's team shapes per size class and writes
+    the fastest to the shape cache (``lsvd_autotune_f64``); returns the
+    per-class report."""
+    ctx = ctx or default_context()
+    buf = C.create_string_buffer(4096)
+    st = ctx.lib.lsvd_autotune_f64(ctx.handle, per_class, cache_path.encode() if cache_path else None,
+                                   C.cast(buf, C.c_void_p), len(buf))
+    _check(ctx.lib, ctx.handle, st, "autotune")
+    return buf.value.decode()
+
+
+def class_shapes(precision: str = "fp64", ctx: Context | None = None) -> np.ndarray:
+    """The (warps, tile, lanes per pair, matrices per team) of each of the 8
+    size classes the batched planner uses now."""
+    ctx = ctx or default_context()
+    out = np.zeros(32, dtype=np.int32)
+    _check(ctx.lib, ctx.handle, ctx.lib.lsvd_class_shapes(ctx.handle, PRECISIONS[precision], _ptr(out)),
+           "class_shapes")
+    return out.reshape(8, 4)
+
+
 def unpack(ns, packed, square: bool = True):
     """Splits a packed buffer into per-matrix arrays."""
     ns = np.asarray(ns, dtype=np.int64)

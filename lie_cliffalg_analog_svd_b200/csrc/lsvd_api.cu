@@ -3,6 +3,8 @@
 // C ABI declared in include/lsvd.h.
 #include <cuda_runtime.h>
 
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -623,6 +625,164 @@ static BatchPlan* pipe_plan(lsvd_context* ctx, int slot, int64_t count, const in
         return nullptr;
     }
     return P.get();
+}
+
+// ----------------------------------------------------------- autotuner ----
+//
+// For every size class of the FP64 batched kernel (n = 5..64), times each
+// feasible team shape -- warps per team {1, 2, 4, 8}, GEMM register tile
+// {2, 4}, lanes per Jacobi pair {8, 16, 32}, matrices per team {1, 2}, with
+// the CTA's teams fitting in 227 KB of shared memory -- on a seeded batch of
+// `per_class` matrices spread over the class's sizes (CUDA events on the
+// context's stream, best of three after one untimed run), keeps the fastest,
+// and writes the choice to the cache that lsvd_autotune_shapes reads.
+static void lcg_gauss(uint64_t& st, double* out, size_t count) {
+    for (size_t i = 0; i < count; i += 2) {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        const double u1 = double((st >> 11) + 1) * (1.0 / 9007199254740993.0);
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        const double u2 = double(st >> 11) * (1.0 / 9007199254740992.0);
+        const double r = std::sqrt(-2.0 * std::log(u1)), t = 6.283185307179586 * u2;
+        out[i] = r * std::cos(t);
+        if (i + 1 < count) out[i + 1] = r * std::sin(t);
+    }
+}
+
+extern "C" lsvd_status lsvd_autotune_f64(lsvd_context* ctx, int64_t per_class, const char* cache_path,
+                                         char* report, int64_t report_cap) {
+    if (!ctx) return LSVD_BAD_ARGUMENT;
+    if (per_class < 16 || per_class > 100000)
+        return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_autotune_f64: per_class in 16..100000");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    cudaError_t e;
+    ClassShape best[kMaxClasses];
+    for (int c = 0; c < kMaxClasses; ++c) best[c] = lsvd_default_shape(c);
+    std::string rep;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "autotune events");
+    lsvd_status out = LSVD_OK;
+    uint64_t seed = 0x5eed1234abcdull;
+    for (int c = 1; c < kMaxClasses && out == LSVD_OK; ++c) {
+        const int lo = kClassHi[c - 1] + 1, hi = kClassHi[c];
+        if (lo > hi) continue;
+        std::vector<int32_t> ns(static_cast<size_t>(per_class));
+        int64_t elems = 0, selems = 0;
+        for (int64_t t = 0; t < per_class; ++t) {
+            ns[size_t(t)] = lo + int(t % (hi - lo + 1));
+            elems += int64_t(ns[size_t(t)]) * ns[size_t(t)];
+            selems += ns[size_t(t)];
+        }
+        std::vector<double> ha(static_cast<size_t>(elems));
+        lcg_gauss(seed, ha.data(), ha.size());
+        double* dA = static_cast<double*>(ctx->ws_a.get(size_t(elems) * 8, &e));
+        double* dU = e == cudaSuccess ? static_cast<double*>(ctx->ws_u.get(size_t(elems) * 8, &e)) : nullptr;
+        double* dS = e == cudaSuccess ? static_cast<double*>(ctx->ws_s.get(size_t(selems) * 8, &e)) : nullptr;
+        double* dV = e == cudaSuccess ? static_cast<double*>(ctx->ws_vt.get(size_t(elems) * 8, &e)) : nullptr;
+        if (e != cudaSuccess ||
+            (e = cudaMemcpyAsync(dA, ha.data(), ha.size() * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+            out = lsvd_ctx_cuda(ctx, e, "autotune batch");
+            break;
+        }
+        double t_best = 1e30, t_def = -1.0;
+        const ClassShape def = lsvd_default_shape(c);
+        std::vector<ClassShape> cands;
+        for (int w : {1, 2, 4, 8})
+            for (int ts : {2, 4})
+                for (int g : {8, 16, 32})
+                    for (int pt : {1, 2})
+                        if (size_t(kCtaThreads / (32 * w)) * team_smem_doubles(hi, w) * 8 <= 227 * 1024)
+                            cands.push_back(ClassShape{w, ts, g, pt});
+        for (const ClassShape& cand : cands) {
+            ClassShape shapes[kMaxClasses];
+            for (int k = 0; k < kMaxClasses; ++k) shapes[k] = lsvd_default_shape(k);
+            shapes[c] = cand;
+            BatchPlan P;
+            if ((out = build_plan(ctx, per_class, ns.data(), shapes, LSVD_PREC_FP64, P)) != LSVD_OK) break;
+            double t = 1e30;
+            for (int rep_i = 0; rep_i < 4; ++rep_i) {
+                float ms = 0.f;
+                if ((e = cudaEventRecord(e0, st)) != cudaSuccess) break;
+                if ((out = lsvd_run_plan(ctx, P, dA, dU, dS, dV, nullptr, false, false)) != LSVD_OK) break;
+                if ((e = cudaEventRecord(e1, st)) != cudaSuccess || (e = cudaEventSynchronize(e1)) != cudaSuccess ||
+                    (e = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess)
+                    break;
+                if (rep_i > 0) t = std::min(t, double(ms));
+            }
+            if (out == LSVD_OK && e != cudaSuccess) out = lsvd_ctx_cuda(ctx, e, "autotune timing");
+            if (out != LSVD_OK) break;
+            if (cand.nwarps == def.nwarps && cand.ts == def.ts && cand.g == def.g && cand.per_team == def.per_team)
+                t_def = t;
+            if (t < t_best) {
+                t_best = t;
+                best[c] = cand;
+            }
+        }
+        if (out != LSVD_OK) break;
+        char line[200];
+        std::snprintf(line, sizeof(line), "class %d (n %d..%d): %d,%d,%d,%d %.3f ms (default %d,%d,%d,%d %.3f ms)\n",
+                      c, lo, hi, best[c].nwarps, best[c].ts, best[c].g, best[c].per_team, t_best, def.nwarps, def.ts,
+                      def.g, def.per_team, t_def);
+        rep += line;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (out != LSVD_OK) return out;
+    // write the cache: keep a "shapes" entry for every precision, replace "shapes_fp64"
+    std::string path = cache_path ? std::string(cache_path) : lsvd_autotune_cache_path();
+    std::string tuned;
+    for (int c = 1; c < kMaxClasses; ++c) {
+        char b[48];
+        std::snprintf(b, sizeof(b), "%s%d:%d,%d,%d,%d", tuned.empty() ? "" : ";", c, best[c].nwarps, best[c].ts,
+                      best[c].g, best[c].per_team);
+        tuned += b;
+    }
+    std::string shared;
+    if (FILE* f = std::fopen(path.c_str(), "r")) {
+        char buf[4096] = {0};
+        const size_t got = std::fread(buf, 1, sizeof(buf) - 1, f);
+        std::fclose(f);
+        buf[got] = 0;
+        if (const char* q = std::strstr(buf, "\"shapes\": \"")) {
+            const char* end = std::strchr(q + 11, '"');
+            if (end) shared.assign(q + 11, end);
+        }
+    }
+    const size_t slash = path.find_last_of('/');
+    if (slash != std::string::npos && slash > 0) {  // create the parent directories
+        const std::string dir = path.substr(0, slash);
+        for (size_t i = 1; i <= dir.size(); ++i)
+            if (i == dir.size() || dir[i] == '/') mkdir(dir.substr(0, i).c_str(), 0755);
+    }
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_autotune_f64: cannot write " + path);
+    std::fprintf(f, "{\"shapes_fp64\": \"%s\"%s%s%s, \"per_class\": %lld, \"sms\": %d}\n", tuned.c_str(),
+                 shared.empty() ? "" : ", \"shapes\": \"", shared.c_str(), shared.empty() ? "" : "\"",
+                 static_cast<long long>(per_class), ctx->num_sms);
+    std::fclose(f);
+    // plans built under the old shapes are stale now
+    ctx->plans.clear();
+    for (auto& pp : ctx->pipe_plans) pp.reset();
+    if (report && report_cap > 0) std::snprintf(report, size_t(report_cap), "%s", rep.c_str());
+    return LSVD_OK;
+}
+
+// The team shapes the planner would use now for `precision` (LSVD_SHAPES, the
+// autotune cache, the defaults): out[4 c + {0..3}] = warps, tile, lanes per
+// pair, matrices per team of class c (8 classes).
+extern "C" lsvd_status lsvd_class_shapes(lsvd_context* ctx, lsvd_precision precision, int32_t* out) {
+    if (!ctx || !out) return LSVD_BAD_ARGUMENT;
+    ClassShape shapes[kMaxClasses];
+    lsvd_autotune_shapes(ctx, precision, shapes);
+    for (int c = 0; c < kMaxClasses; ++c) {
+        out[4 * c] = shapes[c].nwarps;
+        out[4 * c + 1] = shapes[c].ts;
+        out[4 * c + 2] = shapes[c].g;
+        out[4 * c + 3] = shapes[c].per_team;
+    }
+    return LSVD_OK;
 }
 
 // Host-pointer batches of at least kPipeMin matrices are cut into kPipeChunks

@@ -3,8 +3,9 @@
 // The batched planner asks for one ClassShape per size class.  Shapes come,
 // in order of preference, from (1) the LSVD_SHAPES environment variable
 // ("cls:nwarps,ts,g,per_team;..."), (2) the JSON cache written by
-// lsvd_autotune_f64 (LSVD_AUTOTUNE_CACHE, default
-// $HOME/.cache/lsvd_b200/shapes.json), (3) the built-in defaults.
+// lsvd_autotune_f64 (lsvd_api.cu; path LSVD_AUTOTUNE_CACHE, default
+// $HOME/.cache/lsvd_b200/shapes.json): the "shapes_fp64" entry for the FP64
+// kernel, a "shapes" entry for every precision, (3) the built-in defaults.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -32,7 +33,7 @@ static bool parse_shapes(const char* s, ClassShape* shapes) {
     return any;
 }
 
-static std::string cache_path() {
+std::string lsvd_autotune_cache_path() {
     if (const char* p = std::getenv("LSVD_AUTOTUNE_CACHE")) return p;
     const char* home = std::getenv("HOME");
     return std::string(home ? home : "/tmp") + "/.cache/lsvd_b200/shapes.json";
@@ -46,13 +47,15 @@ void lsvd_autotune_shapes(lsvd_context* /*ctx*/, lsvd_precision prec, ClassShape
         shapes[3] = ClassShape{4, 2, 8, 1};
         shapes[4] = ClassShape{4, 4, 8, 1};
     }
-    // cache: a single line {"shapes": "cls:w,ts,g,pt;..."}
-    if (FILE* f = std::fopen(cache_path().c_str(), "r")) {
-        char buf[1024] = {0};
+    // cache: one line {"shapes_fp64": "cls:w,ts,g,pt;...", ...}
+    if (FILE* f = std::fopen(lsvd_autotune_cache_path().c_str(), "r")) {
+        char buf[4096] = {0};
         size_t got = std::fread(buf, 1, sizeof(buf) - 1, f);
         std::fclose(f);
         buf[got] = 0;
         if (const char* q = std::strstr(buf, "\"shapes\": \"")) parse_shapes(q + 11, shapes);
+        if (prec == LSVD_PREC_FP64)
+            if (const char* q = std::strstr(buf, "\"shapes_fp64\": \"")) parse_shapes(q + 16, shapes);
     }
     if (const char* env = std::getenv("LSVD_SHAPES")) parse_shapes(env, shapes);
     shapes[0].nwarps = 0;  // micro class is always thread-per-matrix

@@ -136,3 +136,4 @@ lsvd_status lsvd_large_solve(lsvd_context* ctx, int64_t rows, int64_t cols, cons
 
 // lsvd_autotune.cu
 void lsvd_autotune_shapes(lsvd_context* ctx, lsvd_precision prec, ClassShape* shapes);
+std::string lsvd_autotune_cache_path();
