@@ -65,11 +65,13 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision comparisons added to the batched line")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="batched workload on N GPUs: weak = a full batch per rank; strong = one "
                          "batch split into cost-balanced contiguous shards")
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "polar", "jade", "single", "adjoint"])
+                    choices=["batched", "polar", "jade", "single", "adjoint", "svd_large"])
     ap.add_argument("--families", type=int, default=512)
     ap.add_argument("--polar-size", default="full", choices=["full", "small"],
                     help="small: 2048x2048 and 4096x1024 instead of 4096x4096 and 8192x2048")
@@ -399,8 +401,12 @@ def run_b200(args):
             "data": "synthetic",
             "config": batched_config(args, ws),
             "accuracy": acc, "roofline": roof, "gpu_launches": launches,
-            "clocks": clk.summary(), "e2e": e2e,
-            "polar_tflops": None}
+            "clocks": clk.summary(), "e2e": e2e}
+    if not args.no_mixed and args.precision == "fp64":
+        line["mixed_batched"] = mixed_batched_compare(torch, ctx, stream, ns, ad, sig, out, value / ws, diag, args)
+        line["svd_large"] = large_svd_compare(torch, ctx, device, args.seed + 17 + rank)
+        pp = line["svd_large"]["per_precision"]
+        line["polar_tflops"] = {k: pp[k]["polar_tflops"] for k in ("fp64", "tf32", "bf16")}
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(ns, a, args.cpu_seconds, args.seed)
     if rank == 0:
@@ -408,6 +414,63 @@ def run_b200(args):
     if ws > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+KAPPA_BANDS = [(1.0, 1e2), (1e2, 1e5), (1e5, 1e8), (1e8, 1e13)]
+
+
+def kappa_bands(ns, sig, diag):
+    """Mean Jacobi sweeps and Newton-Schulz iterations per condition-number
+    band (kappa = s_1 / s_n of the imposed spectrum; micro route excluded)."""
+    first = np.concatenate([[0], np.cumsum(ns)[:-1]])
+    last = first + ns - 1
+    kappa = sig[first] / np.maximum(sig[last], 1e-300)
+    out = []
+    for lo, hi in KAPPA_BANDS:
+        sel = (kappa >= lo) & (kappa < hi) & (ns > 4)
+        out.append({"kappa": [lo, hi], "matrices": int(sel.sum()),
+                    "mean_sweeps": float(diag["jacobi_sweeps"][sel].mean()) if sel.any() else None,
+                    "mean_ns_iters": float(diag["ns_iters"][sel].mean()) if sel.any() else None})
+    return out
+
+
+def mixed_batched_compare(torch, ctx, stream, ns, ad, sig, out, fp64_value, fp64_diag, args):
+    """The batched workload through the TF32 and BF16 tensor-core paths
+    (Newton-Schulz bulk in low precision, FP64 refinement and Jacobi cleanup):
+    device-timed SVDs/s, speed-up over the FP64 line, accuracy against the
+    imposed spectra, and the FP64 sweeps per condition-number band."""
+    from lie_cliffalg_analog_svd_b200 import _lib as L
+    from lie_cliffalg_analog_svd_b200 import svd_batched
+    from lie_cliffalg_analog_svd_b200.api import packed_offsets
+    _, so = packed_offsets(ns)
+    res = {"fp64_sweeps_by_kappa": kappa_bands(ns, sig, fp64_diag)}
+    steps = max(2, args.steps // 2)
+    for prec in ("tf32", "bf16"):
+        with torch.cuda.stream(stream):
+            u, s, vt, dg, st = svd_batched(ns, ad, precision=prec, want_diag=True, ctx=ctx, out=out)
+        torch.cuda.synchronize()
+        d = np.frombuffer(dg.cpu().numpy().tobytes(), dtype=L.DIAG_DTYPE)
+        sh = s.cpu().numpy()
+        err = max(float(np.max(np.abs(sh[so[t]:so[t + 1]] - sig[so[t]:so[t + 1]])) / sig[so[t]])
+                  for t in range(ns.size))
+        for _ in range(2):
+            svd_batched(ns, ad, precision=prec, ctx=ctx, out=out, device_async=True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            svd_batched(ns, ad, precision=prec, ctx=ctx, out=out, device_async=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        v = ns.size / (ms * 1e-3)
+        res[prec] = {"value": v, "unit": "SVDs/s", "ms_per_step": ms, "speedup_vs_fp64": v / fp64_value,
+                     "status": int(st), "sigma_err_normwise_max": err,
+                     "orth_u_max": float(d["orth_u"].max()), "orth_v_max": float(d["orth_v"].max()),
+                     "rel_recon_max": float(d["rel_recon"].max()),
+                     "fp64_cleanup_sweeps_by_kappa": kappa_bands(ns, sig, d)}
+    return res
 
 
 # ------------------------------------------------------- other workloads ----
@@ -574,6 +637,203 @@ def run_polar(args):
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.destroy_process_group()
+    return 0
+
+
+def large_inputs(torch, device, seed, shapes, kappas=POLAR_KAPPAS):
+    """SVD inputs of the mixed-precision workload, built on the device: A =
+    Q1 diag(s) Q2^T with Q1 (m x n), Q2 (n x n) from QR of seeded Gaussians and
+    s geometric from 1 to 1/kappa.  Returns [(shape, kappa, A, s)]."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    out = []
+    for (m, n) in shapes:
+        for kappa in kappas:
+            q1 = torch.linalg.qr(torch.randn(m, n, generator=g, device=device, dtype=torch.float64))[0]
+            q2 = torch.linalg.qr(torch.randn(n, n, generator=g, device=device, dtype=torch.float64))[0]
+            sv = kappa ** (-torch.arange(n, device=device, dtype=torch.float64) / (n - 1))
+            out.append(((m, n), kappa, ((q1 * sv) @ q2.T).contiguous(), sv))
+            del q1, q2
+    return out
+
+
+def large_accuracy(r, sv):
+    i = r.info
+    return {"status": int(r.status), "sigma_err_normwise": float((r.s - sv).abs().max() / sv[0]),
+            "orth_u": i.orth_u, "orth_v": i.orth_v, "rel_recon": i.rel_recon,
+            "ns_iters_lowp": i.ns_iters_lowp, "ns_iters_fp64": i.ns_iters_fp64,
+            "sweeps_precond": i.sweeps_lowp, "sweeps_fp64": i.sweeps_fp64,
+            "ms_total": i.ms_total, "ms_polar": i.ms_polar, "ms_eig_precond": i.ms_eig_lowp,
+            "ms_eig_fp64": i.ms_eig_fp64, "flops_fp64": i.flops_fp64, "flops_lowp": i.flops_lowp}
+
+
+def large_svd_compare(torch, ctx, device, seed, shape=(4096, 4096), kappa=1e5):
+    """One matrix of the mixed-precision workload through every precision:
+    device time (CUDA events inside the call), accuracy against the imposed
+    spectrum, the speed-up of each mixed route over the FP64 route, and the
+    Newton-Schulz phase's TFLOP/s (4 m n^2 per iteration)."""
+    from lie_cliffalg_analog_svd_b200 import svd_large
+    (_, _, a, sv), = large_inputs(torch, device, seed, [shape], [kappa])
+    res = {}
+    for prec in ("fp64", "tf32", "bf16"):
+        svd_large(a, prec, want_diag=False, ctx=ctx)  # warm (workspace, graph capture)
+        r = svd_large(a, prec, want_diag=True, ctx=ctx)
+        res[prec] = large_accuracy(r, sv)
+    m, n = shape
+    for prec in ("fp64", "tf32", "bf16"):
+        r = res[prec]
+        it = r["ns_iters_fp64"] if prec == "fp64" else r["ns_iters_lowp"]
+        r["polar_tflops"] = 4.0 * m * n * n * it / (r["ms_polar"] * 1e-3) / 1e12 if r["ms_polar"] > 0 else None
+        if prec != "fp64":
+            r["speedup_vs_fp64"] = res["fp64"]["ms_total"] / r["ms_total"]
+    return {"shape": list(shape), "kappa": kappa, "per_precision": res,
+            "polar_note": "polar_tflops = 4 m n^2 per Newton-Schulz iteration / polar-phase time; the mixed "
+                          "polar phase alone is not FP64-accurate -- at equal accuracy the mixed polar factor "
+                          "is U V^T of the mixed SVD, i.e. the mixed SVD's time"}
+
+
+def run_svd_large(args):
+    """Config 3 as SVDs: 16 dense matrices per step, 4096x4096 and 8192x2048
+    alternating, kappa cycling over 1e2, 1e5, 1e8, through lsvd_svd_large_f64
+    in the requested precision; every input is first solved in FP64, TF32 and
+    BF16 (untimed) for the accuracy table and the per-precision speed-ups."""
+    torch, ws, rank, local, device = _init_dist()
+    from lie_cliffalg_analog_svd_b200 import Context, svd_large
+    ctx = Context(local)
+    stream = torch.cuda.Stream(device)
+    ctx.set_stream(stream.cuda_stream)
+    shapes = POLAR_SHAPES if args.polar_size == "full" else [(2048, 2048), (4096, 1024)]
+    inputs = large_inputs(torch, device, args.seed + rank, shapes)
+    torch.cuda.synchronize()
+    table = []
+    for (shape, kappa, a, sv) in inputs:
+        row = {"shape": list(shape), "kappa": kappa}
+        for prec in ("fp64", "tf32", "bf16"):
+            r = svd_large(a, prec, want_diag=True, ctx=ctx)
+            row[prec] = large_accuracy(r, sv)
+        for prec in ("tf32", "bf16"):
+            row[prec]["speedup_vs_fp64"] = row["fp64"]["ms_total"] / row[prec]["ms_total"]
+        table.append(row)
+    fp64_peak = fp64_peak_tflops(torch, device)
+    order = [inputs[(t % 2) * 3 + (t // 2) % 3] for t in range(POLAR_COUNT)]
+
+    def step():
+        fl = 0.0
+        for (_, _, a, _) in order:
+            fl += svd_large(a, args.precision, want_diag=False, ctx=ctx).info.flops_fp64
+        return fl
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = ctx.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    flops = 0.0
+    with ClockSampler(local) as clk:
+        time.sleep(0.4)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            flops += step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        time.sleep(0.2)
+    ms = _max_over_ranks(torch, ws, device, e0.elapsed_time(e1) / args.steps)
+    launches = ctx.kernel_launches - launches0
+    value = ws * POLAR_COUNT / (ms * 1e-3)
+    # e2e: host (pinned) A in, host U, S, Vt out, through the C ABI
+    import ctypes as C
+    from lie_cliffalg_analog_svd_b200 import _lib as L
+    prec = {"fp64": 0, "tf32": 1, "bf16": 2}[args.precision]
+    pinned = {}
+    for (shape, kappa, a, _) in inputs:
+        m, n = shape
+        h = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        h.copy_(a)
+        pinned[id(a)] = (h.numpy(), torch.empty((m, n), dtype=torch.float64, pin_memory=True).numpy(),
+                         torch.empty(n, dtype=torch.float64, pin_memory=True).numpy(),
+                         torch.empty((n, n), dtype=torch.float64, pin_memory=True).numpy())
+    info = L.LargeInfo()
+
+    def e2e_step():
+        for (_, _, a, _) in order:
+            ah, uh, sh, vh = pinned[id(a)]
+            m, n = ah.shape
+            st = ctx.lib.lsvd_svd_large_f64(ctx.handle, m, n, ah.ctypes.data, n, uh.ctypes.data, n,
+                                            sh.ctypes.data, vh.ctypes.data, n, prec, C.byref(info), 0)
+            assert st in (0, 1), st
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    el = _max_over_ranks(torch, ws, device, (time.perf_counter() - t0) / args.steps)
+    bin_ = sum(a.numel() * 8 for (_, _, a, _) in order)
+    bout = sum((a.shape[0] * a.shape[1] + a.shape[1] + a.shape[1] ** 2) * 8 for (_, _, a, _) in order)
+    achieved = flops / args.steps / (ms * 1e-3) / 1e12
+    wl = "|".join(f"{m}x{n}" for m, n in shapes)
+    line = _base_line(args, "SVDs/s", value, ms, ws, f"svd_large_16x({wl})_kappa1e2-1e8",
+                      {"matrices_per_step": POLAR_COUNT, "shapes": shapes, "kappas": POLAR_KAPPAS,
+                       "precision": args.precision,
+                       "route": "fp64: Newton-Schulz + blocked two-sided Jacobi on P + U = QV; "
+                                "tf32/bf16: tensor-core Newton-Schulz bulk, preconditioning eigensolve to "
+                                "the low-precision level, FP64 one-sided Jacobi on A V0",
+                       "l2": "inputs of 134 MB each, 6 distinct, larger than the 126 MB L2",
+                       "parallelism": f"dp{ws} (independent matrices)"},
+                      "f64" if args.precision == "fp64" else f"{args.precision}+f64")
+    line.update({"accuracy_and_speedup": table,
+                 "roofline": {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": fp64_peak,
+                              "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+                              "kernel": "whole solve: lsvd::dg::dgemm_kernel and the block-Jacobi kernels",
+                              "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul f64) measured in this run",
+                              "flops": "executed FP64 flops counted by the library (info.flops_fp64)"},
+                 "gpu_launches": launches, "clocks": clk.summary(),
+                 "e2e": {"value": ws * POLAR_COUNT / el, "unit": "SVDs/s", "h2d_bytes_per_step": bin_,
+                         "d2h_bytes_per_step": bout, "ms_per_step": el * 1e3}})
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_reference_svd_large(args):
+    """The oracle's LieSvdSmall::solve (single-threaded, like the reference)
+    on square kappa = 1e5 inputs of growing size for about --cpu-seconds; the
+    rate at 4096 x 4096 is extrapolated from the largest size timed by the n^3
+    cost of the solve (stated in the sample)."""
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    O = _oracle()
+    from lie_cliffalg_analog_svd_b200 import profiles as P
+    done, last = [], None
+    n, el = 128, 0.0
+    while n <= 512 and el < args.cpu_seconds:
+        a, _ = P.conditioned_matrix(n, n, 1e5, seed=n)
+        t0 = time.perf_counter()
+        O.LieSvdSmall.solve(a)
+        dt = time.perf_counter() - t0
+        el += dt
+        done.append(f"{n}^2 {dt:.2f} s")
+        last = (n, dt)
+        n *= 2
+    n0, dt0 = last
+    t4096 = dt0 * (4096 / n0) ** 3
+    v = 1.0 / t4096
+    shapes = POLAR_SHAPES if args.polar_size == "full" else [(2048, 2048), (4096, 1024)]
+    wl = "|".join(f"{m}x{n}" for m, n in shapes)
+    line = _base_line(args, "SVDs/s", v, t4096 * 1e3, 1, f"svd_large_16x({wl})_kappa1e2-1e8",
+                      {"matrices_per_step": POLAR_COUNT, "shapes": shapes, "kappas": POLAR_KAPPAS,
+                       "precision": args.precision, "parallelism": "dp1 (independent matrices)"}, "f64")
+    line.update({"impl": "reference",
+                 "cpu_baseline": {"value": v, "unit": "SVDs/s", "cores": 1, "kind": "port",
+                                  "sample": "oracle LieSvdSmall::solve on kappa=1e5 matrices " + ", ".join(done)
+                                            + f"; 4096^2 extrapolated as {dt0:.2f} s x (4096/{n0})^3"},
+                 "e2e": {"value": v, "unit": "SVDs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "note": "a 4096^2 solve of the single-threaded CPU restatement takes hours: timed at the "
+                         "sizes listed and scaled by n^3"})
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -980,9 +1240,9 @@ def main():
     if args.impl == "reference":
         return {"batched": run_reference, "polar": run_reference_polar,
                 "jade": run_reference_jade, "single": run_reference_single,
-                "adjoint": run_reference_adjoint}[args.workload](args)
+                "adjoint": run_reference_adjoint, "svd_large": run_reference_svd_large}[args.workload](args)
     return {"batched": run_b200, "polar": run_polar, "jade": run_jade,
-            "single": run_single, "adjoint": run_adjoint}[args.workload](args)
+            "single": run_single, "adjoint": run_adjoint, "svd_large": run_svd_large}[args.workload](args)
 
 
 if __name__ == "__main__":

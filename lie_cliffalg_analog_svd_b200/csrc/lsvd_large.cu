@@ -702,6 +702,16 @@ __global__ void gather_u_kernel(const double* H, int64_t ldh, int m, int k, cons
         }
 }
 
+// X <- 1.5 X - 0.5 Y on the m x n part of X and Y (leading dimension ld):
+// one Newton-Schulz step X (3I - X^T X) / 2 once Y = X (X^T X).
+__global__ void ns_step_kernel(int m, int n, double* X, const double* Y, int64_t ld) {
+    const int64_t tot = int64_t(m) * n;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = e / n, j = e % n;
+        X[i * ld + j] = 1.5 * X[i * ld + j] - 0.5 * Y[i * ld + j];
+    }
+}
+
 __global__ void frob2_part_kernel(int m, int n, const double* A, int64_t lda, double* part) {
     __shared__ double red[256];
     double s = 0.0;
@@ -1268,6 +1278,30 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
         gather_u_kernel<<<dim3(64, 32), 256, 0, st>>>(H1, ldh1, int(m), int(n), perm_d, sig2, Ud, ld);
         if ((e = cudaStreamSynchronize(st)) != cudaSuccess)  // `inv` is pageable host memory
             return lsvd_ctx_cuda(ctx, e, "large: gather");
+        // W's columns are orthogonal to the normwise scale only: columns with
+        // sigma_j << sigma_1 keep cosines up to ~tol sigma_1 / sigma_j.  FP64
+        // Newton-Schulz steps U <- U (3I - U^T U) / 2 (quadratic) restore
+        // orthonormal columns; X (Q0, no longer needed) holds U (U^T U).
+        for (int it = 0; it < 6; ++it) {
+            if ((e = lsvd::dg::dgemm(st, true, false, int(n), int(n), int(m), 1.0, Ud, ld, Ud, ld, 0.0, Pm, ld)) !=
+                cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: U^T U");
+            diff2_kernel<<<1024, 256, 0, st>>>(int(n), int(n), Pm, ld, nullptr, 0, part);
+            sum_parts_kernel<<<1, 256, 0, st>>>(1024, part, dsum);
+            double o2 = 0.0;
+            if ((e = cudaMemcpyAsync(&o2, dsum, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(st)) != cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: U orthogonality");
+            li.flops_fp64 += 2.0 * double(m) * double(n) * double(n);
+            ctx->launches += 3;
+            if (!(std::sqrt(o2) > 1e-14 * std::sqrt(double(n)))) break;
+            if ((e = lsvd::dg::dgemm(st, false, false, int(m), int(n), int(n), 1.0, Ud, ld, Pm, ld, 0.0, X, ld)) !=
+                cudaSuccess)
+                return lsvd_ctx_cuda(ctx, e, "large: U (U^T U)");
+            ns_step_kernel<<<2048, 256, 0, st>>>(int(m), int(n), Ud, X, ld);
+            li.flops_fp64 += 2.0 * double(m) * double(n) * double(n);
+            ctx->launches += 2;
+        }
     } else {
         gather_vt_kernel<<<2048, 256, 0, st>>>(Vc, npad, 0, int(n), perm_d, Vd, ld);
     }
