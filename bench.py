@@ -419,18 +419,27 @@ def run_b200(args):
 KAPPA_BANDS = [(1.0, 1e2), (1e2, 1e5), (1e5, 1e8), (1e8, 1e13)]
 
 
-def kappa_bands(ns, sig, diag):
+def kappa_bands(ns, sig, diag, packed=False):
     """Mean Jacobi sweeps and Newton-Schulz iterations per condition-number
-    band (kappa = s_1 / s_n of the imposed spectrum; micro route excluded)."""
+    band (kappa = s_1 / s_n of the imposed spectrum; micro route excluded).
+    The mixed kernels pack two counters per field (low precision x 1000 +
+    FP64): `packed` splits them."""
     first = np.concatenate([[0], np.cumsum(ns)[:-1]])
     last = first + ns - 1
     kappa = sig[first] / np.maximum(sig[last], 1e-300)
+    sw = diag["jacobi_sweeps"].astype(np.int64)
+    it = diag["ns_iters"].astype(np.int64)
     out = []
     for lo, hi in KAPPA_BANDS:
         sel = (kappa >= lo) & (kappa < hi) & (ns > 4)
-        out.append({"kappa": [lo, hi], "matrices": int(sel.sum()),
-                    "mean_sweeps": float(diag["jacobi_sweeps"][sel].mean()) if sel.any() else None,
-                    "mean_ns_iters": float(diag["ns_iters"][sel].mean()) if sel.any() else None})
+        mean = (lambda x: float(x[sel].mean()) if sel.any() else None)  # noqa: E731
+        row = {"kappa": [lo, hi], "matrices": int(sel.sum())}
+        if packed:
+            row.update({"mean_sweeps_lowp": mean(sw // 1000), "mean_sweeps_fp64": mean(sw % 1000),
+                        "mean_ns_iters_lowp": mean(it // 1000), "mean_ns_iters_fp64": mean(it % 1000)})
+        else:
+            row.update({"mean_sweeps": mean(sw), "mean_ns_iters": mean(it)})
+        out.append(row)
     return out
 
 
@@ -469,7 +478,7 @@ def mixed_batched_compare(torch, ctx, stream, ns, ad, sig, out, fp64_value, fp64
                      "status": int(st), "sigma_err_normwise_max": err,
                      "orth_u_max": float(d["orth_u"].max()), "orth_v_max": float(d["orth_v"].max()),
                      "rel_recon_max": float(d["rel_recon"].max()),
-                     "fp64_cleanup_sweeps_by_kappa": kappa_bands(ns, sig, d)}
+                     "sweeps_by_kappa": kappa_bands(ns, sig, d, packed=True)}
     return res
 
 

