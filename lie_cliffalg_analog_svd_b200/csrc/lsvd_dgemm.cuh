@@ -7,8 +7,9 @@
 //   op(A) = A   (A row-major M x K, lda >= K)   or A^T (A row-major K x M)
 //   op(B) = B   (B row-major K x N, ldb >= N)   or B^T (B row-major N x K)
 //
-// One CTA of 8 warps computes a 128 x 128 tile; warps are arranged 4 (M) x 2
-// (N) and own 32 x 64 each (4 x 8 tiles of 8 x 8, 64 accumulators a lane).
+// One CTA of 8 warps computes a 128 x 128 tile (or 128 x 64 when the product
+// has too few 128 x 128 tiles to fill the GPU twice); warps are arranged 4 (M)
+// x 2 (N) and own 32 x 64 (32 x 32) each (4 x 8 (4 x 4) tiles of 8 x 8).
 // Operands stream through a 4-stage cp.async ring of BK = 16; each operand
 // tile sits in shared memory either K-contiguous (leading dimension 20
 // doubles) or M/N-contiguous (leading dimension 132 doubles), both = 4 mod 16,
@@ -47,16 +48,17 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-// Loads the BK-slice starting at k0 of a 128-wide operand tile (rows/cols
-// [r0, r0 + 128) of op(X)) into shared memory.  KCONT: the operand's K index
-// is contiguous in global memory (A not transposed, or B transposed).
-template <bool KCONT>
+// Loads the BK-slice starting at k0 of an R-wide operand tile (rows/cols
+// [r0, r0 + R) of op(X), R = 128 or 64) into shared memory.  KCONT: the
+// operand's K index is contiguous in global memory (A not transposed, or B
+// transposed).
+template <bool KCONT, int R = 128>
 __device__ __forceinline__ void load_tile(double* sm, const double* X, int64_t ldx, int r0, int rdim,
                                           int k0, int kdim, int tid) {
     if (KCONT) {
-        // 128 rows x 16 k = 1024 chunks of two doubles
+        // R rows x 16 k = 8 R chunks of two doubles
 #pragma unroll
-        for (int it = 0; it < 4; ++it) {
+        for (int it = 0; it < R / 32; ++it) {
             const int c = tid + it * THREADS;
             const int row = c >> 3, kc = (c & 7) * 2;
             const int gr = r0 + row, gk = k0 + kc;
@@ -67,11 +69,11 @@ __device__ __forceinline__ void load_tile(double* sm, const double* X, int64_t l
             cp_async16(sm + row * LDK + kc, src, valid * 8);
         }
     } else {
-        // 16 k-rows x 128 = 1024 chunks
+        // 16 k-rows x R = 8 R chunks
 #pragma unroll
-        for (int it = 0; it < 4; ++it) {
+        for (int it = 0; it < R / 32; ++it) {
             const int c = tid + it * THREADS;
-            const int kr = c >> 6, mc = (c & 63) * 2;
+            const int kr = c / (R / 2), mc = (c % (R / 2)) * 2;
             const int gk = k0 + kr, gm = r0 + mc;
             int valid = rdim - gm;
             valid = valid > 2 ? 2 : (valid < 0 ? 0 : valid);
@@ -99,25 +101,26 @@ struct GemmArgs {
     double alpha, beta;
 };
 
-template <bool TA, bool TB>
+template <bool TA, bool TB, int TBN = BN>
 __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(const GemmArgs g) {
+    constexpr int WJ = TBN / 16;  // 8 x 8 tiles per warp along N
     extern __shared__ __align__(16) double dsm[];
     // A's K is contiguous when A is not transposed; B's when B is transposed
     constexpr bool AK = !TA, BKC = TB;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp >> 1, wn = warp & 1;
     const int gq = lane >> 2, q = lane & 3;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * TBN;
     const double* A = g.A + int64_t(blockIdx.z) * g.strideA;
     const double* B = g.B + int64_t(blockIdx.z) * g.strideB;
     double* Cz = g.C + int64_t(blockIdx.z) * g.strideC;
     const int KT = (g.K + BK - 1) / BK;
 
-    double acc[4][8][2];
+    double acc[4][WJ][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < WJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
     auto sa = [&](int s) { return dsm + s * 2 * TILE_DOUBLES; };
     auto sb = [&](int s) { return dsm + s * 2 * TILE_DOUBLES + TILE_DOUBLES; };
@@ -125,7 +128,7 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(const GemmArgs g) {
     for (int s = 0; s < STAGES - 1; ++s) {
         if (s < KT) {
             load_tile<AK>(sa(s), A, g.lda, m0, g.M, s * BK, g.K, tid);
-            load_tile<BKC>(sb(s), B, g.ldb, n0, g.N, s * BK, g.K, tid);
+            load_tile<BKC, TBN>(sb(s), B, g.ldb, n0, g.N, s * BK, g.K, tid);
         }
         cp_async_commit();
     }
@@ -137,7 +140,7 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(const GemmArgs g) {
             if (nk < KT) {
                 const int s = nk % STAGES;
                 load_tile<AK>(sa(s), A, g.lda, m0, g.M, nk * BK, g.K, tid);
-                load_tile<BKC>(sb(s), B, g.ldb, n0, g.N, nk * BK, g.K, tid);
+                load_tile<BKC, TBN>(sb(s), B, g.ldb, n0, g.N, nk * BK, g.K, tid);
             }
             cp_async_commit();
         }
@@ -145,15 +148,15 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(const GemmArgs g) {
         const double* Bs = sb(kt % STAGES);
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 4) {
-            double a[4], b[8];
+            double a[4], b[WJ];
 #pragma unroll
             for (int i = 0; i < 4; ++i) a[i] = frag<AK>(As, wm * 32 + i * 8 + gq, kk + q);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) b[j] = frag<BKC>(Bs, wn * 64 + j * 8 + gq, kk + q);
+            for (int j = 0; j < WJ; ++j) b[j] = frag<BKC>(Bs, wn * (TBN / 2) + j * 8 + gq, kk + q);
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 8; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+                for (int j = 0; j < WJ; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
     }
     cp_async_wait<0>();
@@ -164,8 +167,8 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(const GemmArgs g) {
         if (r >= g.M) continue;
         double* crow = Cz + int64_t(r) * g.ldc;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int c = n0 + wn * 64 + j * 8 + 2 * q;
+        for (int j = 0; j < WJ; ++j) {
+            const int c = n0 + wn * (TBN / 2) + j * 8 + 2 * q;
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 if (c + e < g.N) {
@@ -188,21 +191,38 @@ inline cudaError_t dgemm(cudaStream_t st, bool ta, bool tb, int M, int N, int K,
         (sA | sB) & 1)
         return cudaErrorInvalidValue;
     GemmArgs g{M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, alpha, beta};
-    const dim3 grid(unsigned((N + BN - 1) / BN), unsigned((M + BM - 1) / BM), unsigned(batch));
+    // 128 x 64 tiles when 128 x 128 tiles would not fill the GPU twice over
+    static int sms = [] {
+        int d = 0, v = 148;
+        if (cudaGetDevice(&d) != cudaSuccess || cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d) != cudaSuccess)
+            v = 148;
+        return v;
+    }();
+    const int64_t tiles = int64_t((N + BN - 1) / BN) * ((M + BM - 1) / BM) * batch;
+    const bool narrow = tiles < 2 * sms;
+    const int bn = narrow ? 64 : BN;
+    const dim3 grid(unsigned((N + bn - 1) / bn), unsigned((M + BM - 1) / BM), unsigned(batch));
     cudaError_t e;
-    if (!ta && !tb) {
-        e = cudaFuncSetAttribute(dgemm_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e == cudaSuccess) dgemm_kernel<false, false><<<grid, THREADS, SMEM_BYTES, st>>>(g);
-    } else if (ta && !tb) {
-        e = cudaFuncSetAttribute(dgemm_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e == cudaSuccess) dgemm_kernel<true, false><<<grid, THREADS, SMEM_BYTES, st>>>(g);
-    } else if (!ta && tb) {
-        e = cudaFuncSetAttribute(dgemm_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e == cudaSuccess) dgemm_kernel<false, true><<<grid, THREADS, SMEM_BYTES, st>>>(g);
-    } else {
-        e = cudaFuncSetAttribute(dgemm_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e == cudaSuccess) dgemm_kernel<true, true><<<grid, THREADS, SMEM_BYTES, st>>>(g);
+#define LSVD_DGEMM_LAUNCH(TA_, TB_)                                                                          \
+    if (narrow) {                                                                                             \
+        e = cudaFuncSetAttribute(dgemm_kernel<TA_, TB_, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                 SMEM_BYTES);                                                                 \
+        if (e == cudaSuccess) dgemm_kernel<TA_, TB_, 64><<<grid, THREADS, SMEM_BYTES, st>>>(g);              \
+    } else {                                                                                                  \
+        e = cudaFuncSetAttribute(dgemm_kernel<TA_, TB_, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                 SMEM_BYTES);                                                                 \
+        if (e == cudaSuccess) dgemm_kernel<TA_, TB_, BN><<<grid, THREADS, SMEM_BYTES, st>>>(g);              \
     }
+    if (!ta && !tb) {
+        LSVD_DGEMM_LAUNCH(false, false)
+    } else if (ta && !tb) {
+        LSVD_DGEMM_LAUNCH(true, false)
+    } else if (!ta && tb) {
+        LSVD_DGEMM_LAUNCH(false, true)
+    } else {
+        LSVD_DGEMM_LAUNCH(true, true)
+    }
+#undef LSVD_DGEMM_LAUNCH
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }

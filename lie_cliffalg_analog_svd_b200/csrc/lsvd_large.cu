@@ -13,7 +13,7 @@
 // The eigensolve is eigh_jacobi_full (:212-285) blocked for the GPU: indices
 // are grouped in blocks of 32, and round-robin layers (the circle method of
 // layer_pairs, src/lie_svd_joint.rs:524-539) pair the blocks.  Per sweep the
-// reference's start-of-sweep test off(P) < 1e-13 ||P||_F (offnorm_kernel);
+// reference's start-of-sweep test off(P) < 1e-13 ||P||_F (offnorm_part_kernel, offnorm_final_kernel);
 // per layer
 //   solve2_kernel   diagonalises the 64 x 64 diagonal block of every block
 //                   pair by cyclic Jacobi sweeps (Rutishauser tangent,
@@ -150,6 +150,8 @@ __global__ void __launch_bounds__(256) gram_kernel(const double* __restrict__ H,
         }
 }
 
+// Maximum over the CTA's NT threads (same value on every thread); red >= NT / 32.
+template <int NT>
 __device__ __forceinline__ double block_max(double v, double* red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -157,7 +159,7 @@ __device__ __forceinline__ double block_max(double v, double* red) {
     __syncthreads();
     double r = 0.0;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) r = fmax(r, red[w]);
+    for (int w = 0; w < NT / 32; ++w) r = fmax(r, red[w]);
     __syncthreads();
     return r;
 }
@@ -178,14 +180,14 @@ __device__ __forceinline__ double pair_scale(double mii, double mjj, double S) {
 // Gram in shared memory.
 __device__ __forceinline__ double scaled_offdiag(const double* Ms, double S, double* red) {
     double off = 0.0;
-    for (int e = threadIdx.x; e < PW * PW; e += 256) {
+    for (int e = threadIdx.x; e < PW * PW; e += 256) {  // 256-thread CTAs
         const int i = e >> 6, j = e & 63;
         if (i < j) {
             const double d = pair_scale(Ms[i * MLD + i], Ms[j * MLD + j], S);
             if (d > 0.0) off = fmax(off, fabs(Ms[i * MLD + j]) / d);
         }
     }
-    return block_max(off, red);
+    return block_max<256>(off, red);
 }
 
 // Cyclic two-sided Jacobi sweeps (at most inner_max, parallel round-robin
@@ -194,7 +196,7 @@ __device__ __forceinline__ double scaled_offdiag(const double* Ms, double S, dou
 // decides whether pair (p, q) is rotated; the sweeps stop after one in which
 // no pair was.  Returns the sweeps run (inner_max + 1 when the cap was hit)
 // and adds the rotations to *cnt.
-template <class Rot>
+template <int NT, class Rot>
 __device__ int inner_jacobi(double* Ms, double* Rs, int inner_max, Rot rotate, double* cs, double* sn, int* pa,
                             int* qa, int* flag, int* cnt) {
     const int tid = threadIdx.x;
@@ -233,7 +235,7 @@ __device__ int inner_jacobi(double* Ms, double* Rs, int inner_max, Rot rotate, d
             }
             __syncthreads();
             // M <- J^T M J over 32 x 32 independent 2 x 2 blocks
-            for (int b = tid; b < 32 * 32; b += 256) {
+            for (int b = tid; b < 32 * 32; b += NT) {
                 const int ka = b >> 5, kb = b & 31;
                 const double ca = cs[ka], sa = sn[ka], cb = cs[kb], sb = sn[kb];
                 if (sa == 0.0 && sb == 0.0) continue;
@@ -251,7 +253,7 @@ __device__ int inner_jacobi(double* Ms, double* Rs, int inner_max, Rot rotate, d
                 Ms[rb * MLD + cb_] = w2;
             }
             // R <- R J
-            for (int t = tid; t < PW * 32; t += 256) {
+            for (int t = tid; t < PW * 32; t += NT) {
                 const int r = t >> 5, k = t & 31;
                 const double c = cs[k], s = sn[k];
                 if (s == 0.0) continue;
@@ -296,7 +298,7 @@ __global__ void __launch_bounds__(256) solve_kernel(const double* __restrict__ M
     {
         double dmax = 0.0;
         for (int i = tid; i < PW; i += 256) dmax = fmax(dmax, Ms[i * MLD + i]);
-        dmax = block_max(dmax, red);
+        dmax = block_max<256>(dmax, red);
         if (tid == 0)
             atomicMax(&stt->next_scale2, static_cast<unsigned long long>(__double_as_longlong(dmax)));
     }
@@ -306,7 +308,7 @@ __global__ void __launch_bounds__(256) solve_kernel(const double* __restrict__ M
         if (tid == 0) skip[pair] = 1;
         return;
     }
-    const int sw = inner_jacobi(
+    const int sw = inner_jacobi<256>(
         Ms, Rs, inner_max,
         [&](double app, double aqq, double apq) { return fabs(apq) > tol * pair_scale(app, aqq, S); }, cs, sn,
         pa, qa, &s_flag, &s_cnt);
@@ -326,38 +328,57 @@ __device__ __forceinline__ int pair_index(int c, int P, int Q) { return hrow_of(
 // Two-sided route, sweep start: off(P)^2 = sum_{p<q} P_pq^2 over the
 // symmetric P (npad x npad, row-major); the solve stops before the sweep when
 // sqrt(off) < tol_ref ||P0||_F -- the test eigh_jacobi_full makes at the start
-// of every sweep (src/lie_svd_small.rs:220-228).  One CTA.
-__global__ void __launch_bounds__(1024) offnorm_kernel(const double* __restrict__ P, int64_t ldp, int n,
-                                                       SweepState* __restrict__ stt, double limit) {
+// of every sweep (src/lie_svd_small.rs:220-228).  Partial sums per CTA, then
+// one CTA adds them and sets the flag.
+__global__ void __launch_bounds__(256) offnorm_part_kernel(const double* __restrict__ P, int64_t ldp, int n,
+                                                           const SweepState* __restrict__ stt,
+                                                           double* __restrict__ part) {
     if (stt->converged) return;
-    __shared__ double red[32];
+    __shared__ double red[8];
     double s = 0.0;
-    const int64_t tot = int64_t(n) * n;
-    for (int64_t e = threadIdx.x; e < tot; e += 1024) {
-        const int64_t i = e / n, j = e % n;
-        if (i < j) {
-            const double v = P[i * ldp + j];
+    // rows i = blockIdx.x + k gridDim.x, the upper triangle of each row
+    for (int i = blockIdx.x; i < n; i += gridDim.x)
+        for (int j = i + 1 + threadIdx.x; j < n; j += 256) {
+            const double v = P[int64_t(i) * ldp + j];
             s += v * v;
         }
-    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
-        for (int w = 0; w < 32; ++w) t += red[w];
-        const double off = sqrt(t);
+        for (int w = 0; w < 8; ++w) t += red[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void offnorm_final_kernel(const double* __restrict__ part, int nparts, SweepState* __restrict__ stt,
+                                     double limit) {
+    if (stt->converged) return;
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += 256) s += part[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double off = sqrt(red[0]);
         stt->last_off = off;
         if (off < limit) stt->converged = 1;
     }
 }
 
-// Two-sided route: gathers the 64 x 64 diagonal block of block pair
-// blockIdx.x from P, diagonalises it (rotations of |a_pq| > tau, the
+// Two-sided route (1024 threads: the 63 rounds of a block sweep are the
+// critical path of every layer, so each round's 32 x 32 two-sided 2 x 2
+// updates take one per thread): gathers the 64 x 64 diagonal block of block
+// pair blockIdx.x from P, diagonalises it (rotations of |a_pq| > tau, the
 // reference rotating every |a_pq| >= 1e-300, src/lie_svd_small.rs:233-235),
 // and writes R / skip like solve_kernel.
-__global__ void __launch_bounds__(256) solve2_kernel(const double* __restrict__ P, int64_t ldp, int nb, int layer,
+__global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__ P, int64_t ldp, int nb, int layer,
                                                      double* __restrict__ Rg, int* __restrict__ skip,
                                                      SweepState* __restrict__ stt, double tau, int inner_max) {
     if (stt->converged) return;
@@ -366,12 +387,12 @@ __global__ void __launch_bounds__(256) solve2_kernel(const double* __restrict__ 
     double* Rs = ssmem + PW * MLD;
     __shared__ double cs[32], sn[32];
     __shared__ int pa[32], qa[32];
-    __shared__ double red[8];
+    __shared__ double red[32];
     __shared__ int s_cnt, s_flag;
     const int pair = blockIdx.x, tid = threadIdx.x;
     int Pb, Qb;
     block_pair(nb, layer, pair, Pb, Qb);
-    for (int e = tid; e < PW * PW; e += 256) {
+    for (int e = tid; e < PW * PW; e += 1024) {
         const int i = e >> 6, j = e & 63;
         Ms[i * MLD + j] = P[int64_t(pair_index(i, Pb, Qb)) * ldp + pair_index(j, Pb, Qb)];
         Rs[i * MLD + j] = i == j ? 1.0 : 0.0;
@@ -379,20 +400,20 @@ __global__ void __launch_bounds__(256) solve2_kernel(const double* __restrict__ 
     if (tid == 0) s_cnt = 0;
     __syncthreads();
     double off = 0.0;
-    for (int e = tid; e < PW * PW; e += 256) {
+    for (int e = tid; e < PW * PW; e += 1024) {
         const int i = e >> 6, j = e & 63;
         if (i < j) off = fmax(off, fabs(Ms[i * MLD + j]));
     }
-    off = block_max(off, red);
+    off = block_max<1024>(off, red);
     if (!(off > tau)) {
         if (tid == 0) skip[pair] = 1;
         return;
     }
-    const int sw = inner_jacobi(
+    const int sw = inner_jacobi<1024>(
         Ms, Rs, inner_max, [&](double, double, double apq) { return fabs(apq) > tau; }, cs, sn, pa, qa, &s_flag,
         &s_cnt);
     double* R = Rg + int64_t(pair) * (PW * PW);
-    for (int e = tid; e < PW * PW; e += 256) R[e] = Rs[(e >> 6) * MLD + (e & 63)];
+    for (int e = tid; e < PW * PW; e += 1024) R[e] = Rs[(e >> 6) * MLD + (e & 63)];
     if (tid == 0) {
         skip[pair] = 0;
         stt->rotated = 1;
@@ -928,7 +949,7 @@ static lsvd_status run_sweeps(lsvd_context* ctx, double* H, int64_t ldh, int gm,
 
 // Blocked two-sided Jacobi on the symmetric P (npad x npad, row-major, padding
 // zero) accumulating V into Vc (row j = v_j; I on entry): per sweep the
-// reference's start-of-sweep test off(P) < limit (offnorm_kernel), then for
+// reference's start-of-sweep test off(P) < limit (offnorm_part_kernel, offnorm_final_kernel), then for
 // every round-robin layer the block solves (solve2_kernel), P <- R^T P R
 // (twoside_kernel) and V <- V R (apply_kernel on Vc).
 static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, int npad, double limit, double tau,
@@ -952,7 +973,8 @@ static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, 
     skip2[0] = reinterpret_cast<int*>(p); p += al(size_t(npairs) * 4);
     skip2[1] = reinterpret_cast<int*>(p); p += al(size_t(npairs) * 4);
     Rg2[0] = reinterpret_cast<double*>(p); p += al(size_t(npairs) * PW * PW * 8);
-    Rg2[1] = reinterpret_cast<double*>(p);
+    Rg2[1] = reinterpret_cast<double*>(p); p += al(size_t(npairs) * PW * PW * 8);
+    double* offpart = reinterpret_cast<double*>(p);  // 256 partial sums of the off-norm test
     cudaError_t e = cudaMemsetAsync(stt, 0, sizeof(SweepState), st);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(solve2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem);
@@ -978,12 +1000,13 @@ static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, 
         destroy_events();
         return lsvd_ctx_cuda(ctx, e, "large: begin capture");
     }
-    offnorm_kernel<<<1, 1024, 0, st>>>(P, npad, n, stt, limit);
+    offnorm_part_kernel<<<256, 256, 0, st>>>(P, npad, n, stt, offpart);
+    offnorm_final_kernel<<<1, 256, 0, st>>>(offpart, 256, stt, limit);
     for (int layer = 0; layer < nb - 1; ++layer) {
         const int b = layer & 1;
         // the buffers of parity b were last read by V's update two layers back
         if (layer >= 2) cudaStreamWaitEvent(st, evs[2 + b], 0);
-        solve2_kernel<<<npairs, 256, kSolveSmem, st>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt, tau, inner_max);
+        solve2_kernel<<<npairs, 1024, kSolveSmem, st>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt, tau, inner_max);
         cudaEventRecord(evs[0], st);
         cudaStreamWaitEvent(sv, evs[0], 0);
         apply_kernel<<<dim3(npairs, napply), 256, kApplySmem, sv>>>(Vc, npad, nb, layer, rows, Rg2[b], skip2[b], stt);
@@ -1003,7 +1026,7 @@ static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, 
     e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: graph instantiate");
-    const int launches_per_sweep = 3 * (nb - 1) + 2;
+    const int launches_per_sweep = 3 * (nb - 1) + 3;
     SweepState* hst = static_cast<SweepState*>(lsvd_ctx_pinned(ctx, 2 * sizeof(SweepState)));
     cudaEvent_t ev[2] = {nullptr, nullptr};
     lsvd_status out = LSVD_OK;
@@ -1061,7 +1084,7 @@ static size_t sweep_ws_bytes(int gpad, int npad, int num_sms) {
     // state | skip x 2 | rotations x 2 | Gram partials (the two-sided route uses the second
     // skip and rotation buffers, the one-sided route the partials)
     return al(sizeof(SweepState)) + 2 * al(size_t(npairs) * 4) + 2 * al(size_t(npairs) * PW * PW * 8) +
-           al(size_t(npairs) * (nchunk + 1) * PW * PW * 8);
+           al(256 * 8) + al(size_t(npairs) * (nchunk + 1) * PW * PW * 8);
 }
 
 static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,

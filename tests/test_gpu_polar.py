@@ -44,8 +44,9 @@ def _round_bf16(x: np.ndarray) -> np.ndarray:
 
 @pytest.mark.parametrize("ta,tb", [(False, False), (True, False), (False, True), (True, True)])
 @pytest.mark.parametrize("M,N,K", [(128, 128, 16), (1, 1, 1), (7, 9, 5), (130, 257, 33), (300, 200, 1000),
-                                   (512, 384, 4096), (64, 1000, 3)])
+                                   (512, 384, 4096), (64, 1000, 3), (2560, 2312, 96)])
 def test_gemm_f64(ta, tb, M, N, K):
+    # the small shapes run on 128 x 64 tiles, (2560, 2312, 96) on 128 x 128 tiles
     import torch
     rng = np.random.default_rng(M * 13 + N * 5 + K + 2 * ta + tb)
     a = rng.standard_normal((K, M) if ta else (M, K))
