@@ -960,3 +960,288 @@ int64_t oracle_svd_batch(int64_t count, const int32_t* idx, const int32_t* n, co
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------- triage --
+// Test infrastructure: restatement of the reference's triage statistics, the
+// checker of lsvd_triage_batched_f64.
+
+struct VecPhase {  // VectorPhaseHealth (src/lie_svd_phasehealth.rs:21-40)
+    double scalar_mean, scalar_sq, vector_sq, delay_bivector_sq, gradient_sq, energy_entropy, twist_ratio, phase;
+};
+
+// analyze_vector_phase_by (src/lie_svd_phasehealth.rs:146-207) and
+// normalized_energy_entropy_by (:313-329) over x(0..n-1).
+template <class F>
+static VecPhase vector_phase(int64_t n, F at) {
+    VecPhase h{0, 0, 0, 0, 0, 0, 0, 0};
+    if (n == 0) return h;
+    const double nf = double(n);
+    double sum = 0.0;
+    for (int64_t i = 0; i < n; ++i) sum += at(i);
+    const double mean = sum / nf;
+    h.scalar_mean = mean;
+    h.scalar_sq = nf * mean * mean;
+    double vector_sq = 0.0, norm_sq = 0.0, delay = 0.0, grad = 0.0, energy = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double xi = at(i), xn = at((i + 1) % n);
+        const double c = xi - mean;
+        vector_sq += c * c;
+        norm_sq += xi * xi;
+        delay += xi * xn;
+        const double d = xn - xi;
+        grad += d * d;
+        energy += xi * xi;
+    }
+    h.vector_sq = vector_sq;
+    h.delay_bivector_sq = std::max(norm_sq * norm_sq - delay * delay, 0.0);
+    h.gradient_sq = grad;
+    double ent = 0.0;
+    if (n > 1 && energy > 1e-300) {
+        for (int64_t i = 0; i < n; ++i) {
+            const double v = at(i);
+            const double pr = (v * v) / energy;
+            if (pr > 0.0) ent -= pr * std::log(pr);
+        }
+        ent /= std::log(nf);
+    }
+    h.energy_entropy = ent;
+    h.twist_ratio = std::sqrt(h.delay_bivector_sq) / std::max(norm_sq, 1e-300);
+    const double orient = delay >= 0.0 ? 1.0 : -1.0;
+    h.phase = orient * std::atan2(std::sqrt(grad), std::fabs(mean) + std::sqrt(vector_sq) + 1e-300);
+    return h;
+}
+
+struct PhaseSummary {  // PhaseHealthSummary via summarize (:274-311)
+    double dbsq = 0.0, gsq = 0.0, max_twist = 0.0, mean_twist = 0.0, mean_entropy = 0.0;
+    int64_t count = 0;
+};
+
+// global_phase_invariants' weighted phase sums (:219-232), rows then columns
+struct PhaseSums {
+    double sin_w = 0.0, cos_w = 0.0, w = 0.0;
+};
+
+static void add_item(PhaseSummary& s, PhaseSums& g, const VecPhase& h) {
+    s.dbsq += h.delay_bivector_sq;
+    s.gsq += h.gradient_sq;
+    s.max_twist = std::max(s.max_twist, h.twist_ratio);
+    s.mean_twist += h.twist_ratio;
+    s.mean_entropy += h.energy_entropy;
+    s.count += 1;
+    const double w = std::sqrt(h.scalar_sq + h.vector_sq);
+    g.sin_w += w * std::sin(h.phase);
+    g.cos_w += w * std::cos(h.phase);
+    g.w += w;
+}
+
+static void finish(PhaseSummary& s) {
+    if (s.count) {
+        s.mean_twist /= double(s.count);
+        s.mean_entropy /= double(s.count);
+    }
+}
+
+// analyze_block4_signature(..).dual_balance (src/lie_svd_block4.rs:210-262).
+static double block4_dual_balance(int64_t rows, int64_t cols, const double* A) {
+    const int64_t n = std::min(rows, cols), blocks = n / 4;
+    if (blocks == 0) return 0.0;
+    double sd2 = 0.0, asd2 = 0.0;
+    auto w = [&](int64_t st, int a, int b) { return 0.5 * (A[(st + b) * cols + st + a] - A[(st + a) * cols + st + b]); };
+    const double r = 0.70710678118654752440;  // 1/sqrt(2)
+    for (int64_t blk = 0; blk < blocks; ++blk) {
+        const int64_t st = blk * 4;
+        const double w12 = w(st, 0, 1), w13 = w(st, 0, 2), w14 = w(st, 0, 3);
+        const double w23 = w(st, 1, 2), w24 = w(st, 1, 3), w34 = w(st, 2, 3);
+        const double sd[3] = {(w12 + w34) * r, (w13 - w24) * r, (w14 + w23) * r};
+        const double asd[3] = {(w12 - w34) * r, (w13 + w24) * r, (w14 - w23) * r};
+        sd2 += sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2];
+        asd2 += asd[0] * asd[0] + asd[1] * asd[1] + asd[2] * asd[2];
+    }
+    const double a = std::sqrt(sd2), b = std::sqrt(asd2);
+    return std::fabs(a - b) / std::max(a + b, 1e-300);
+}
+
+static double coeff_var(const std::vector<double>& v) {  // src/lie_svd_adaptive.rs:341-355
+    double sum = 0.0;
+    for (double x : v) sum += x;
+    const double len = double(std::max<size_t>(v.size(), 1));
+    const double mean = sum / len;
+    if (std::fabs(mean) <= 1e-300) return 0.0;
+    double var = 0.0;
+    for (double x : v) var += (x - mean) * (x - mean);
+    return std::sqrt(var / len) / std::fabs(mean);
+}
+
+static double rel_l2_mismatch(const std::vector<double>& a, const std::vector<double>& b) {  // :357-366
+    double num = 0.0, den = 0.0;
+    for (size_t i = 0; i < a.size(); ++i) {
+        const double d = a[i] - b[i];
+        num += d * d;
+        den += a[i] * a[i] + b[i] * b[i];
+    }
+    return std::sqrt(num) / std::max(std::sqrt(den), 1e-300);
+}
+
+static double entropy01(const std::vector<double>& v) {  // :368-380
+    double sum = 0.0;
+    for (double x : v) sum += x;
+    if (sum <= 1e-300 || v.size() <= 1) return 1.0;
+    double h = 0.0;
+    for (double x : v) {
+        const double pr = x / sum;
+        if (pr > 0.0) h -= pr * std::log(pr);
+    }
+    return h / std::max(std::log(double(v.size())), 1e-300);
+}
+
+extern "C" {
+
+int oracle_triage(int64_t rows, int64_t cols, const double* A, double* out, int32_t* routes) {
+    if (rows < 0 || cols < 0) return -1;
+    const int64_t n = rows, m = cols;
+    // phase signature (src/lie_svd_phasehealth.rs:100-140) and global invariants (:213-272)
+    PhaseSummary R, Cs;
+    PhaseSums g;
+    for (int64_t i = 0; i < n; ++i) add_item(R, g, vector_phase(m, [&](int64_t j) { return A[i * m + j]; }));
+    for (int64_t j = 0; j < m; ++j) add_item(Cs, g, vector_phase(n, [&](int64_t i) { return A[i * m + j]; }));
+    finish(R);
+    finish(Cs);
+    const double count = double(std::max<int64_t>(R.count + Cs.count, 1));
+    const double total_stress = std::sqrt(R.dbsq + Cs.dbsq) + std::sqrt(R.gsq + Cs.gsq);
+    const double mean_stress = total_stress / count;
+    const double max_twist = std::max(R.max_twist, Cs.max_twist);
+    const double entropy_gap = std::fabs(R.mean_entropy - Cs.mean_entropy);
+    const int64_t cor = std::min(n, m);
+    double upper = 0.0, lower = 0.0, torsion = 0.0;
+    for (int64_t i = 0; i < cor; ++i)
+        for (int64_t j = i + 1; j < cor; ++j) {  // triangular_disbalance (:331-343)
+            upper += A[i * m + j] * A[i * m + j];
+            lower += A[j * m + i] * A[j * m + i];
+        }
+    const double causal = std::fabs(upper - lower) / std::max(upper + lower, 1e-300);
+    for (int64_t i = 0; i < cor; ++i)
+        for (int64_t j = i + 1; j < cor; ++j) {
+            const double d = (A[i * m + j] - A[j * m + i]) * 0.5;
+            torsion += 2.0 * d * d;
+        }
+    const double global_phase = g.w > 1e-300 ? std::atan2(g.sin_w, g.cos_w) : 0.0;
+    double total_sq = 0.0;
+    for (int64_t e = 0; e < n * m; ++e) total_sq += A[e] * A[e];
+    double pent = 0.0;
+    if (n * m > 1 && total_sq > 1e-300) {
+        for (int64_t e = 0; e < n * m; ++e) {
+            const double pr = (A[e] * A[e]) / total_sq;
+            if (pr > 0.0) pent -= pr * std::log(pr);
+        }
+        pent /= std::log(double(n * m));
+    }
+    // PhaseEngine passport extras: real_chirality (src/lie_svd_engine.rs:277-292), golden_resonance_real (:310-326)
+    double skew = 0.0, tot = 0.0;
+    for (int64_t i = 0; i < cor; ++i)
+        for (int64_t j = 0; j < cor; ++j) {
+            const double x = A[i * m + j];
+            tot += x * x;
+            if (i < j) {
+                const double d = A[i * m + j] - A[j * m + i];
+                skew += d * d;
+            }
+        }
+    const double chirality = std::sqrt(skew) / std::max(std::sqrt(tot), 1e-300);
+    const double theta = 2.39996322972865332;
+    double re = 0.0, im = 0.0, mass = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double ph = theta * double(i);
+        double rm = 0.0;
+        for (int64_t j = 0; j < m; ++j) rm += std::fabs(A[i * m + j]);
+        re += rm * std::cos(ph);
+        im += rm * std::sin(ph);
+        mass += rm;
+    }
+    const double golden = std::sqrt(re * re + im * im) / std::max(mass, 1e-300);
+    const double nan = std::nan("");
+    for (int k = 0; k < 11; ++k) out[k] = nan;
+    out[11] = mean_stress;
+    out[12] = max_twist;
+    out[13] = causal;
+    out[14] = entropy_gap;
+    out[15] = global_phase;
+    out[16] = std::sqrt(torsion);
+    out[17] = block4_dual_balance(n, m, A);
+    out[18] = pent;
+    out[19] = chirality;
+    out[20] = golden;
+    // passport route hint (src/lie_svd_engine.rs:75-82)
+    routes[1] = (n == m && (max_twist > 0.8 || causal > 0.65 || entropy_gap > 0.2) && n <= 128) ? 1 : 0;
+    routes[0] = -1;
+    if (n != m) return 0;
+    // analyze_matrix (src/lie_svd_adaptive.rs:186-274)
+    double all_sq = 0.0, diag_sq = 0.0, off_sq = 0.0, sym_sq = 0.0, skew_sq = 0.0;
+    std::vector<double> dabs(size_t(n), 0.0), rl1(size_t(n), 0.0), cl1(size_t(n), 0.0), rl2(size_t(n), 0.0),
+        cl2(size_t(n), 0.0);
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t j = 0; j < n; ++j) {
+            const double v = A[i * n + j], av = std::fabs(v);
+            all_sq += v * v;
+            rl1[size_t(i)] += av;
+            cl1[size_t(j)] += av;
+            rl2[size_t(i)] += v * v;
+            cl2[size_t(j)] += v * v;
+            if (i == j) {
+                diag_sq += v * v;
+                dabs[size_t(i)] = av;
+            } else {
+                off_sq += v * v;
+            }
+        }
+    for (int64_t i = 0; i < n; ++i) {
+        rl2[size_t(i)] = std::sqrt(rl2[size_t(i)]);
+        cl2[size_t(i)] = std::sqrt(cl2[size_t(i)]);
+        for (int64_t j = i + 1; j < n; ++j) {
+            const double a = A[i * n + j], b = A[j * n + i];
+            const double sy = 0.5 * (a + b), sk = 0.5 * (a - b);
+            sym_sq += 2.0 * sy * sy;
+            skew_sq += 2.0 * sk * sk;
+        }
+    }
+    const double norm = std::max(std::sqrt(all_sq), 1e-300);
+    const double offdiag = std::sqrt(off_sq) / norm, dd = std::sqrt(diag_sq) / norm;
+    const double rcv = coeff_var(rl2), ccv = coeff_var(cl2), mism = rel_l2_mismatch(rl1, cl1);
+    const double symr = std::sqrt(sym_sq) / std::max(std::sqrt(sym_sq + skew_sq), 1e-300);
+    const double torr = std::sqrt(skew_sq) / std::max(std::sqrt(sym_sq + skew_sq), 1e-300);
+    const double dent = entropy01(dabs), rent = entropy01(rl1), cent = entropy01(cl1);
+    // suspicious_score (:325-339)
+    double score = 0.0;
+    score += std::max(offdiag - 0.55, 0.0) * 0.9;
+    score += std::max(0.35 - dd, 0.0) * 0.8;
+    score += std::max(rcv, ccv) * 1.4;
+    score += mism * 1.6;
+    score += torr * 0.45;
+    score += offdiag * std::max(symr - 0.82, 0.0) * 1.8;
+    score += std::max(0.78 - dent, 0.0) * 1.2;
+    const double vals[11] = {offdiag, dd, rcv, ccv, mism, symr, torr, dent, rent, cent, score};
+    for (int k = 0; k < 11; ++k) out[k] = vals[k];
+    // choose_route with LieSvdAdaptiveParams::default() (:55-65, :103-119, :121-184)
+    const double thr = 1.15;
+    const bool balanced_degenerate = score >= thr + 0.25 && offdiag > 0.90 && dd < 0.25 && rcv >= 0.20 &&
+                                     ccv >= 0.20 && rcv < 0.45 && ccv < 0.45 && mism < 0.45;
+    const bool phaseflow =
+        balanced_degenerate || (causal > 0.88 && offdiag > 0.20 && mean_stress > 1.0) ||
+        (mean_stress > 50.0 && max_twist > 0.92 && rcv < 0.42 && ccv < 0.42 && mism < 0.30 && offdiag > 0.85 &&
+         dd < 0.35) ||
+        (out[17] > 0.30 && offdiag > 0.20 && out[16] > 1.0 && dd < 0.5);
+    const bool symmetric_topological = symr > 0.96 && offdiag > 0.35 && dd < 0.95;
+    const bool coreflow = symmetric_topological || balanced_degenerate ||
+                          (score >= thr && (rent < 0.92 || cent < 0.92) && mism < 0.22 &&
+                           (torr < 0.62 || dent < 0.62) && rcv < 0.42 && ccv < 0.42);
+    int route;
+    if (n <= 4) route = 0;
+    else if (offdiag <= 1e-5) route = 1;
+    else if (n <= 64 && phaseflow) route = 2;
+    else if (n <= 64 && coreflow) route = 3;
+    else if (n <= 512) route = 1;
+    else route = 4;
+    routes[0] = route;
+    return 0;
+}
+
+}  // extern "C"

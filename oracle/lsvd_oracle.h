@@ -57,6 +57,22 @@ int64_t oracle_svd_batch(int64_t count, const int32_t* idx, const int32_t* n, co
                          const int64_t* soff, const double* A, double* U, double* S, double* Vt,
                          int32_t threads);
 
+/* Triage of one rows x cols matrix: LieSvdAdaptive's analyze_matrix and
+ * choose_route (src/lie_svd_adaptive.rs:84-274, default params), the
+ * PhaseSignature of lie_svd_phasehealth::phase_signature (src/
+ * lie_svd_phasehealth.rs:100-343) with its global invariants and the 4x4
+ * block dual balance (src/lie_svd_block4.rs:210-266), and PhaseEngine's
+ * passport extras (src/lie_svd_engine.rs:75-103, :277-326).  out[0..20]:
+ * offdiag_ratio, diagonal_dominance, row_cv, col_cv, row_col_mismatch,
+ * symmetry_ratio, transpose_torsion_ratio, diagonal_entropy,
+ * row_mass_entropy, col_mass_entropy, suspicious_score (NaN unless square),
+ * mean_stress, max_twist, causal_disbalance, entropy_gap, global_phase,
+ * torsion_energy, chirality_balance, phase_entropy, chirality,
+ * golden_resonance; routes[0] = AdaptiveRoute (0 Micro, 1 Small,
+ * 2 PhaseFlow, 3 CoreFlowTopo, 4 Hybrid; -1 not square), routes[1] =
+ * passport PhaseRoute (0 RealSmall, 1 RealPhaseFlowPolished). */
+int oracle_triage(int64_t rows, int64_t cols, const double* A, double* out, int32_t* routes);
+
 /* LieSvdMicro::solve (src/lie_svd_micro.rs:21-52), n in 0..4. */
 int oracle_micro_solve(int64_t n, const double* A, double* U, double* S, double* Vt,
                        oracle_small_info* info);

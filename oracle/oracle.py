@@ -65,6 +65,7 @@ def lib():
         _lib.oracle_joint_svd.argtypes = [C.c_int64, C.c_int64, C.c_int64, P, JointParams, P, P,
                                           P, C.POINTER(JointTrace)]
         V = C.c_void_p
+        _lib.oracle_triage.argtypes = [C.c_int64, C.c_int64, V, V, V]
         _lib.oracle_svd_batch.restype = C.c_int64
         _lib.oracle_svd_batch.argtypes = [C.c_int64, V, V, V, V, V, V, V, V, C.c_int32]
     return _lib
@@ -76,6 +77,33 @@ def _p(a):
 
 def _c(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+TRIAGE_FIELDS = ("offdiag_ratio", "diagonal_dominance", "row_cv", "col_cv", "row_col_mismatch",
+                 "symmetry_ratio", "transpose_torsion_ratio", "diagonal_entropy", "row_mass_entropy",
+                 "col_mass_entropy", "suspicious_score", "mean_stress", "max_twist", "causal_disbalance",
+                 "entropy_gap", "global_phase", "torsion_energy", "chirality_balance", "phase_entropy",
+                 "chirality", "golden_resonance")
+ADAPTIVE_ROUTES = ("Micro", "Small", "PhaseFlow", "CoreFlowTopo", "Hybrid")
+PASSPORT_ROUTES = ("RealSmall", "RealPhaseFlowPolished")
+
+
+def triage(a) -> dict:
+    """Oracle restatement of analyze_matrix / choose_route
+    (src/lie_svd_adaptive.rs:84-274), phase_signature
+    (src/lie_svd_phasehealth.rs:100-343) and the PhaseEngine passport
+    extras (src/lie_svd_engine.rs:75-103): field name -> value, plus
+    "route" (AdaptiveRoute name, None when not square) and "passport_route"."""
+    a = _c(a)
+    rows, cols = a.shape
+    out = np.empty(21)
+    routes = np.zeros(2, dtype=np.int32)
+    v = lambda x: C.c_void_p(x.ctypes.data)  # noqa: E731
+    assert lib().oracle_triage(rows, cols, v(a), v(out), v(routes)) == 0
+    d = dict(zip(TRIAGE_FIELDS, out.tolist()))
+    d["route"] = ADAPTIVE_ROUTES[routes[0]] if routes[0] >= 0 else None
+    d["passport_route"] = PASSPORT_ROUTES[routes[1]]
+    return d
 
 
 def svd_batch(ns, a, idx, threads: int, out=None):
