@@ -300,6 +300,38 @@ LSVD_API lsvd_status lsvd_joint_svd_f64(lsvd_context* ctx, int64_t families, int
                                         double* U, double* sig, double* Vt, lsvd_joint_trace* traces,
                                         uint32_t flags);
 
+/* ----------------------------------------------------------- triage ---- */
+
+/* Routing statistics of one matrix: AdaptiveTriage (src/lie_svd_adaptive.rs:
+ * 14-34; NaN unless square), PhaseSignature with its GlobalPhaseInvariants
+ * (src/lie_svd_phasehealth.rs:42-98) and the PhasePassport extras
+ * (src/lie_svd_engine.rs:34-61). */
+typedef struct lsvd_triage {
+    double offdiag_ratio, diagonal_dominance, row_cv, col_cv, row_col_mismatch;
+    double symmetry_ratio, transpose_torsion_ratio, diagonal_entropy, row_mass_entropy, col_mass_entropy;
+    double suspicious_score;
+    double mean_stress, max_twist, causal_disbalance, entropy_gap;
+    double global_phase, torsion_energy, chirality_balance, phase_entropy;
+    double chirality, golden_resonance;
+    /* choose_route with LieSvdAdaptiveParams::default() (:84-119): 0 Micro,
+     * 1 Small, 2 PhaseFlow, 3 CoreFlowTopo, 4 Hybrid; -1 for non-square */
+    int32_t adaptive_route;
+    /* PhaseEngine::passport_real's route_hint (src/lie_svd_engine.rs:75-82):
+     * 0 RealSmall, 1 RealPhaseFlowPolished */
+    int32_t passport_route;
+} lsvd_triage;
+
+/* Replaces analyze_matrix + choose_route (src/lie_svd_adaptive.rs:84-274),
+ * phase_signature (src/lie_svd_phasehealth.rs:129-140) and the statistics
+ * of PhaseEngine::passport_real (src/lie_svd_engine.rs:75-103) for a batch:
+ * matrix t is rows[t] x cols[t] (each <= 4096), row-major, back to back in
+ * A; out gets one lsvd_triage per matrix.  rows/cols are host memory; A and
+ * out host or device (LSVD_DEVICE_POINTERS); with LSVD_ASYNC and device
+ * pointers the call only enqueues.  One CTA per matrix. */
+LSVD_API lsvd_status lsvd_triage_batched_f64(lsvd_context* ctx, int64_t count, const int32_t* rows,
+                                             const int32_t* cols, const double* A, lsvd_triage* out,
+                                             uint32_t flags);
+
 /* ------------------------------------------------ large polar factor ---- */
 /* Polar factor Q (m x n, Q^T Q = I) of a large dense A (m >= n) by the
  * Newton-Schulz iteration X <- X (3I - X^T X)/2 from X0 = A/||A||_F.

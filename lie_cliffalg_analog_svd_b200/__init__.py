@@ -9,8 +9,10 @@ the first call does, and fails loudly if it was not built.
 from .api import (Context, LieSvd, LieSvdMicro, LieSvdSmall, SmallResult, SvdMetrics,  # noqa: F401
                   HardwareSchedule, JointDiagonalizationParams, LieSvdJoint, default_context,
                   PolarResult, SvdStream, metrics, packed_offsets, polar, svd_batched,
-                  svd_batched_stream, svd_vjp, unpack, svd_large, LargeResult)
+                  svd_batched_stream, svd_vjp, unpack, svd_large, LargeResult,
+                  LieSvdAdaptive, PhaseEngine, triage_batched)
 from ._lib import LsvdError  # noqa: F401
 
 __all__ = ["Context", "HardwareSchedule", "JointDiagonalizationParams", "LieSvdJoint", "LieSvd", "LieSvdMicro", "LieSvdSmall", "SmallResult", "SvdMetrics",
-           "PolarResult", "SvdStream", "svd_batched_stream", "svd_vjp", "default_context", "metrics", "packed_offsets", "polar", "svd_batched", "unpack", "LsvdError", "svd_large", "LargeResult"]
+           "PolarResult", "SvdStream", "svd_batched_stream", "svd_vjp", "default_context", "metrics", "packed_offsets", "polar", "svd_batched", "unpack", "LsvdError", "svd_large", "LargeResult",
+           "LieSvdAdaptive", "PhaseEngine", "triage_batched"]

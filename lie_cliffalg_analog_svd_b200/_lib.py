@@ -63,6 +63,21 @@ class LargeInfo(C.Structure):
                 ("orth_u", C.c_double), ("orth_v", C.c_double)]
 
 
+TRIAGE_FIELDS = ("offdiag_ratio", "diagonal_dominance", "row_cv", "col_cv", "row_col_mismatch",
+                 "symmetry_ratio", "transpose_torsion_ratio", "diagonal_entropy", "row_mass_entropy",
+                 "col_mass_entropy", "suspicious_score", "mean_stress", "max_twist", "causal_disbalance",
+                 "entropy_gap", "global_phase", "torsion_energy", "chirality_balance", "phase_entropy",
+                 "chirality", "golden_resonance")
+
+
+class Triage(C.Structure):
+    _fields_ = [(f, C.c_double) for f in TRIAGE_FIELDS] + [("adaptive_route", C.c_int32),
+                                                             ("passport_route", C.c_int32)]
+
+
+TRIAGE_DTYPE = [(f, "<f8") for f in TRIAGE_FIELDS] + [("adaptive_route", "<i4"), ("passport_route", "<i4")]
+
+
 class LsvdError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"lsvd status {status}: {msg}")
@@ -92,6 +107,7 @@ SIGNATURES = {
     "lsvd_svd_batched_f64": (C.c_int, [P, I64, P, P, P, P, P, P, C.c_int, U32]),
     "lsvd_svd_large_f64": (C.c_int, [P, I64, I64, P, I64, P, I64, P, P, I64, C.c_int, P, U32]),
     "lsvd_autotune_f64": (C.c_int, [P, I64, C.c_char_p, P, I64]),
+    "lsvd_triage_batched_f64": (C.c_int, [P, I64, P, P, P, P, U32]),
     "lsvd_class_shapes": (C.c_int, [P, C.c_int, P]),
     "lsvd_metrics_f64": (C.c_int, [P, I64, I64, I64, P, P, P, P, P, P, U32]),
     "lsvd_svd_batched_noalloc_f64": (C.c_int, [P, I64, P, P, P, P, P, P, U32]),

@@ -250,6 +250,115 @@ class LieSvd:
         return LieSvdSmall.solve(a, ctx=ctx)
 
 
+ADAPTIVE_ROUTES = ("Micro", "Small", "PhaseFlow", "CoreFlowTopo", "Hybrid")
+PASSPORT_ROUTES = ("RealSmall", "RealPhaseFlowPolished")
+
+
+def triage_batched(mats, ctx: Context | None = None) -> np.ndarray:
+    """Routing statistics of every matrix (``lsvd_triage_batched_f64``): a
+    structured array with the AdaptiveTriage, PhaseSignature and passport
+    fields, ``adaptive_route`` and ``passport_route`` per matrix."""
+    ctx = ctx or default_context()
+    mats = [_f64(m) for m in mats]
+    rows = np.array([m.shape[0] for m in mats], dtype=np.int32)
+    cols = np.array([m.shape[1] for m in mats], dtype=np.int32)
+    flat = np.concatenate([m.ravel() for m in mats]) if mats else np.zeros(0)
+    out = np.empty(len(mats), dtype=L.TRIAGE_DTYPE)
+    if len(mats):
+        st = ctx.lib.lsvd_triage_batched_f64(ctx.handle, len(mats), _ptr(rows), _ptr(cols), _ptr(flat),
+                                             _ptr(out), 0)
+        _check(ctx.lib, ctx.handle, st, "triage_batched")
+    return out
+
+
+def _triage_dict(rec) -> dict:
+    d = {f: float(rec[f]) for f in L.TRIAGE_FIELDS}
+    r = int(rec["adaptive_route"])
+    d["route"] = ADAPTIVE_ROUTES[r] if r >= 0 else None
+    d["passport_route"] = PASSPORT_ROUTES[int(rec["passport_route"])]
+    return d
+
+
+class LieSvdAdaptive:
+    """``LieSvdAdaptive``'s triage (src/lie_svd_adaptive.rs:84-274) on the GPU.
+    The routes themselves beyond the exact tiers (PhaseFlow, CoreFlowTopo,
+    Hybrid) are research solvers this library does not provide: ``solve``
+    runs the exact tier (Micro for n <= 4, Small otherwise) and reports the
+    route the reference would have taken."""
+
+    @staticmethod
+    def analyze_matrix(a, ctx: Context | None = None) -> dict:
+        a = _f64(a)
+        if a.ndim != 2 or a.shape[0] != a.shape[1]:
+            raise L.LsvdError(L.BAD_SHAPE, "adaptive SVD expects square matrices")
+        return _triage_dict(triage_batched([a], ctx=ctx)[0])
+
+    @staticmethod
+    def choose_route(a, ctx: Context | None = None) -> str:
+        return LieSvdAdaptive.analyze_matrix(a, ctx=ctx)["route"]
+
+
+@dataclass
+class PhaseEngineReport:
+    passport: dict
+    route: str
+    time_s: float
+    rel_recon: float | None
+    orth_u: float | None
+    orth_v: float | None
+    phase_stress: tuple | None
+    schedule_events: int
+
+
+class PhaseEngine:
+    """``PhaseEngine``'s real-matrix facade (src/lie_svd_engine.rs:75-136,
+    :246-275) over the GPU kernels."""
+
+    @staticmethod
+    def passport_real(a, ctx: Context | None = None) -> dict:
+        a = _f64(a)
+        d = _triage_dict(triage_batched([a], ctx=ctx)[0])
+        d.update({"rows": a.shape[0], "cols": a.shape[1], "family": 1, "tensor_modes": None,
+                  "route_hint": d.pop("passport_route")})
+        return d
+
+    @staticmethod
+    def solve_real(a, ctx: Context | None = None):
+        """``PhaseEngine::solve_real`` for inputs whose passport routes them to
+        ``RealSmall`` (LieSvdSmall::solve on the GPU); the PhaseFlow route is
+        a research solver outside this library and raises LSVD_UNSUPPORTED."""
+        import time
+        a = _f64(a)
+        passport = PhaseEngine.passport_real(a, ctx=ctx)
+        if passport["route_hint"] != "RealSmall":
+            raise L.LsvdError(L.UNSUPPORTED, "PhaseEngine::solve_real: the RealPhaseFlowPolished route is not "
+                                             "provided by this library")
+        t0 = time.perf_counter()
+        u, s, vt = LieSvdSmall.solve(a, ctx=ctx)
+        el = time.perf_counter() - t0
+        m = metrics.compute(a, u, s, vt, ctx=ctx)
+        return (u, s, vt), PhaseEngineReport(passport, "RealSmall", el, m.rel_recon, m.orth_u, m.orth_v, None, 0)
+
+    @staticmethod
+    def diagonalize_family(mats, ctx: Context | None = None):
+        """``PhaseEngine::diagonalize_family``: Phase-JADE of the family on the
+        GPU with the passport of its first matrix."""
+        import time
+        if not len(mats):
+            raise L.LsvdError(L.BAD_SHAPE, "PhaseEngine: empty matrix family")
+        t0 = time.perf_counter()
+        v, diags, trace = LieSvdJoint.diagonalize_symmetric_with_params(
+            mats, JointDiagonalizationParams.for_n(np.asarray(mats[0]).shape[0]), ctx=ctx)
+        el = time.perf_counter() - t0
+        passport = PhaseEngine.passport_real(mats[0], ctx=ctx)
+        passport["family"] = len(mats)
+        passport["route_hint"] = "JointPhaseJade"
+        rep = PhaseEngineReport(passport, "JointPhaseJade", el, None, None,
+                                float(np.linalg.norm(v.T @ v - np.eye(v.shape[1]))),
+                                (trace.initial_offdiag, trace.final_offdiag), int(trace.rotations))
+        return v, diags, trace, rep
+
+
 @dataclass
 class SvdMetrics:
     rel_recon: float
