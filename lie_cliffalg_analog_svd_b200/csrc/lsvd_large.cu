@@ -723,13 +723,25 @@ __global__ void gather_u_kernel(const double* H, int64_t ldh, int m, int k, cons
         }
 }
 
-// X <- 1.5 X - 0.5 Y on the m x n part of X and Y (leading dimension ld):
-// one Newton-Schulz step X (3I - X^T X) / 2 once Y = X (X^T X).
-__global__ void ns_step_kernel(int m, int n, double* X, const double* Y, int64_t ld) {
+// G (n x n, UᵀU) -> F = strictly upper part of G plus half of diag(G) - I/2,
+// so that F + F^T = G - I.  U <- U (I - F) is then Gram-Schmidt to first
+// order: column j only takes out columns i < j (larger singular values), and
+// the departure G - I squares at every step.
+__global__ void gs_factor_kernel(int n, double* G, int64_t ld) {
+    const int64_t tot = int64_t(n) * n;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = e / n, j = e % n;
+        double& g = G[i * ld + j];
+        g = i < j ? g : (i == j ? 0.5 * (g - 1.0) : 0.0);
+    }
+}
+
+// X <- X - Y on the m x n part (leading dimension ld).
+__global__ void sub_kernel(int m, int n, double* X, const double* Y, int64_t ld) {
     const int64_t tot = int64_t(m) * n;
     for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * blockDim.x) {
         const int64_t i = e / n, j = e % n;
-        X[i * ld + j] = 1.5 * X[i * ld + j] - 0.5 * Y[i * ld + j];
+        X[i * ld + j] -= Y[i * ld + j];
     }
 }
 
@@ -1302,10 +1314,14 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
         if ((e = cudaStreamSynchronize(st)) != cudaSuccess)  // `inv` is pageable host memory
             return lsvd_ctx_cuda(ctx, e, "large: gather");
         // W's columns are orthogonal to the normwise scale only: columns with
-        // sigma_j << sigma_1 keep cosines up to ~tol sigma_1 / sigma_j.  FP64
-        // Newton-Schulz steps U <- U (3I - U^T U) / 2 (quadratic) restore
-        // orthonormal columns; X (Q0, no longer needed) holds U (U^T U).
-        for (int it = 0; it < 6; ++it) {
+        // sigma_j << sigma_1 keep cosines up to ~tol sigma_1 / sigma_j.  Gram-
+        // Schmidt in descending sigma order (the order of the reference's MGS
+        // repair, src/lie_svd_small.rs:82-144) restores orthonormal columns and
+        // moves column j by at most its cosines with larger columns, i.e. the
+        // product U S V^T by ~tol sigma_1: U <- U (I - F), F the upper half of
+        // U^T U - I, until ||U^T U - I|| reaches rounding.  X (Q0, no longer
+        // needed) holds U F.
+        for (int it = 0; it < 8; ++it) {
             if ((e = lsvd::dg::dgemm(st, true, false, int(n), int(n), int(m), 1.0, Ud, ld, Ud, ld, 0.0, Pm, ld)) !=
                 cudaSuccess)
                 return lsvd_ctx_cuda(ctx, e, "large: U^T U");
@@ -1318,12 +1334,13 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
             li.flops_fp64 += 2.0 * double(m) * double(n) * double(n);
             ctx->launches += 3;
             if (!(std::sqrt(o2) > 1e-14 * std::sqrt(double(n)))) break;
+            gs_factor_kernel<<<2048, 256, 0, st>>>(int(n), Pm, ld);
             if ((e = lsvd::dg::dgemm(st, false, false, int(m), int(n), int(n), 1.0, Ud, ld, Pm, ld, 0.0, X, ld)) !=
                 cudaSuccess)
-                return lsvd_ctx_cuda(ctx, e, "large: U (U^T U)");
-            ns_step_kernel<<<2048, 256, 0, st>>>(int(m), int(n), Ud, X, ld);
+                return lsvd_ctx_cuda(ctx, e, "large: U F");
+            sub_kernel<<<2048, 256, 0, st>>>(int(m), int(n), Ud, X, ld);
             li.flops_fp64 += 2.0 * double(m) * double(n) * double(n);
-            ctx->launches += 2;
+            ctx->launches += 3;
         }
     } else {
         gather_vt_kernel<<<2048, 256, 0, st>>>(Vc, npad, 0, int(n), perm_d, Vd, ld);
