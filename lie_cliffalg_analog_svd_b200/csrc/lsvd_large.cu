@@ -217,7 +217,8 @@ __device__ int inner_jacobi(double* Ms, double* Rs, int inner_max, Rot rotate, d
                 }
                 const double app = Ms[p * MLD + p], aqq = Ms[qq * MLD + qq], apq = Ms[p * MLD + qq];
                 double c = 1.0, s = 0.0;
-                if (apq != 0.0 && rotate(app, aqq, apq)) {
+                const bool rot = apq != 0.0 && rotate(app, aqq, apq);
+                if (rot) {
                     // Rutishauser's tangent (src/lie_svd_small.rs:235-242)
                     const double zeta = (aqq - app) / (2.0 * apq);
                     const double t = fabs(zeta) > 1e150
@@ -225,7 +226,11 @@ __device__ int inner_jacobi(double* Ms, double* Rs, int inner_max, Rot rotate, d
                                          : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
                     c = rsqrt(1.0 + t * t);
                     s = t * c;
-                    atomicAdd(cnt, 1);
+                }
+                // one count per round instead of a contended shared atomic per rotation
+                const unsigned msk = __ballot_sync(0xffffffffu, rot);
+                if (tid == 0 && msk) {
+                    *cnt += __popc(msk);
                     *flag = 1;
                 }
                 cs[tid] = c;
