@@ -324,17 +324,19 @@ class PhaseEngine:
 
     @staticmethod
     def solve_real(a, ctx: Context | None = None):
-        """``PhaseEngine::solve_real`` for inputs whose passport routes them to
-        ``RealSmall`` (LieSvdSmall::solve on the GPU); the PhaseFlow route is
-        a research solver outside this library and raises LSVD_UNSUPPORTED."""
+        """``PhaseEngine::solve_real``: the passport on the GPU, then the SVD.
+        The ``RealPhaseFlowPolished`` route is a research solver this library
+        does not provide; inputs the passport sends there are solved by the
+        exact route (LieSvdSmall::solve on the GPU) and the report says so
+        (``route`` "RealSmall", ``passport['route_hint']`` unchanged)."""
         import time
         a = _f64(a)
         passport = PhaseEngine.passport_real(a, ctx=ctx)
-        if passport["route_hint"] != "RealSmall":
-            raise L.LsvdError(L.UNSUPPORTED, "PhaseEngine::solve_real: the RealPhaseFlowPolished route is not "
-                                             "provided by this library")
         t0 = time.perf_counter()
-        u, s, vt = LieSvdSmall.solve(a, ctx=ctx)
+        if a.shape[0] == a.shape[1]:
+            u, s, vt = LieSvdSmall.solve(a, ctx=ctx)
+        else:
+            u, s, vt = LieSvdSmall.solve_rectangular(a, ctx=ctx)
         el = time.perf_counter() - t0
         m = metrics.compute(a, u, s, vt, ctx=ctx)
         return (u, s, vt), PhaseEngineReport(passport, "RealSmall", el, m.rel_recon, m.orth_u, m.orth_v, None, 0)

@@ -77,13 +77,16 @@ def test_batched_workload_routes():
 
 def test_phase_engine_facade():  # src/lie_svd_engine.rs:338-362
     (u, s, vt), rep = PhaseEngine.solve_real(np.eye(6))
-    assert rep.passport["rows"] == 6 and rep.rel_recon < 1e-12 and rep.route == "RealSmall"
+    assert rep.passport["rows"] == 6 and rep.rel_recon < 1e-12
+    # the identity's rows all twist (ratio 1): the reference routes it to PhaseFlow,
+    # which this library replaces by the exact route
+    assert rep.passport["route_hint"] == "RealPhaseFlowPolished" and rep.route == "RealSmall"
     pp = PhaseEngine.passport_real(upper_shift(8))
     assert np.isfinite(pp["global_phase"]) and pp["torsion_energy"] > 0
     assert 0 <= pp["chirality_balance"] <= 1 and 0 <= pp["phase_entropy"] <= 1
-    with pytest.raises(L.LsvdError) as ei:  # routed to PhaseFlow: not provided here
-        PhaseEngine.solve_real(upper_shift(24, 1.0, 5.0))
-    assert ei.value.status == L.UNSUPPORTED
+    a = np.random.default_rng(4).standard_normal((40, 40))
+    (u, s, vt), rep = PhaseEngine.solve_real(a)
+    assert rep.passport["route_hint"] == "RealSmall" and rep.rel_recon < 4e-13
     rng = np.random.default_rng(2)
     q = np.linalg.qr(rng.standard_normal((10, 10)))[0]
     fam = [q @ np.diag(1.0 + k + np.arange(10) * 0.3) @ q.T for k in range(4)]
