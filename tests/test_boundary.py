@@ -89,3 +89,37 @@ def test_product_never_imports_the_oracle():
             if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
                 txt = open(os.path.join(dirpath, f)).read()
                 assert not re.search(r"^\s*(import|from)\s+oracle|lsvd_oracle|oracle/", txt, re.M), f
+
+
+def _header_text():
+    txt = open(os.path.join(ROOT, "include", "lsvd.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return re.sub(r"//[^\n]*", "", txt)
+
+
+def test_rust_binding_matches_header():
+    # rust/lie_svd_gpu/src/ffi.rs declares every export with the header's
+    # parameter count, and every struct with the header's fields in order
+    # (the crate is source only: no Rust toolchain here)
+    rs = open(os.path.join(ROOT, "rust", "lie_svd_gpu", "src", "ffi.rs")).read()
+    hdr = _header_text()
+    c_fns = {m.group(1): m.group(2) for m in re.finditer(r"LSVD_API[^;(]*?\b(lsvd_\w+)\s*\(([^)]*)\)\s*;", hdr)}
+    r_fns = {m.group(1): m.group(2) for m in re.finditer(r"pub fn (lsvd_\w+)\s*\(([^)]*)\)", rs)}
+    assert set(r_fns) == set(c_fns) == set(header_functions())
+
+    def arity(args):
+        args = " ".join(args.split())
+        return 0 if args in ("", "void") else args.count(",") + 1
+
+    for name, args in c_fns.items():
+        assert arity(r_fns[name]) == arity(args), name
+    c_structs = {m.group(2): re.findall(r"(\w+)\s*(?:,|;)", m.group(1))
+                 for m in re.finditer(r"typedef struct\s*\w*\s*\{(.*?)\}\s*(\w+);", hdr, flags=re.S)}
+    r_structs = {m.group(1): re.findall(r"pub (\w+):", m.group(2))
+                 for m in re.finditer(r"pub struct (\w+)\s*\{(.*?)\}", rs, flags=re.S)}
+    pairs = {"lsvd_diag": "LsvdDiag", "lsvd_rotor": "LsvdRotor", "lsvd_large_info": "LsvdLargeInfo",
+             "lsvd_joint_params": "LsvdJointParams", "lsvd_joint_trace": "LsvdJointTrace",
+             "lsvd_triage": "LsvdTriage", "lsvd_polar_info": "LsvdPolarInfo"}
+    assert set(pairs) == set(c_structs)
+    for c_name, r_name in pairs.items():
+        assert r_structs[r_name] == c_structs[c_name], c_name

@@ -84,9 +84,16 @@ def test_phase_engine_facade():  # src/lie_svd_engine.rs:338-362
     pp = PhaseEngine.passport_real(upper_shift(8))
     assert np.isfinite(pp["global_phase"]) and pp["torsion_energy"] > 0
     assert 0 <= pp["chirality_balance"] <= 1 and 0 <= pp["phase_entropy"] <= 1
+    # a Gaussian matrix twists like the identity (PhaseFlow hint); a rank-one
+    # outer product does not (RealSmall hint); both hints as the oracle's
     a = np.random.default_rng(4).standard_normal((40, 40))
     (u, s, vt), rep = PhaseEngine.solve_real(a)
-    assert rep.passport["route_hint"] == "RealSmall" and rep.rel_recon < 4e-13
+    assert rep.passport["route_hint"] == O.triage(a)["passport_route"] == "RealPhaseFlowPolished"
+    assert rep.route == "RealSmall" and rep.rel_recon < 4e-13
+    r1 = np.outer(np.arange(1.0, 9.0), np.arange(1.0, 9.0))
+    (u, s, vt), rep = PhaseEngine.solve_real(r1)
+    assert rep.passport["route_hint"] == O.triage(r1)["passport_route"] == "RealSmall"
+    assert rep.rel_recon < 4e-13
     rng = np.random.default_rng(2)
     q = np.linalg.qr(rng.standard_normal((10, 10)))[0]
     fam = [q @ np.diag(1.0 + k + np.arange(10) * 0.3) @ q.T for k in range(4)]
