@@ -441,6 +441,114 @@ LSVD_API lsvd_status lsvd_schedule_from_rotors(const lsvd_rotor* rotors, int64_t
                                                int64_t channels, int32_t target, char* json,
                                                int64_t cap, int64_t* len);
 
+/* One event of the real PhaseFlow route: MziPhase (src/lie_svd_phaseflow.rs:
+ * 202-209); kind = the PhaseRotorKind variant's position (:189-199),
+ * LSVD_ROTOR_KIND_*. */
+typedef struct lsvd_mzi_phase {
+    int64_t pass;
+    int64_t i;
+    int64_t j;
+    double theta_l;
+    double theta_r;
+    int32_t kind;
+    int32_t pad_;
+} lsvd_mzi_phase;
+
+#define LSVD_ROTOR_KIND_GOLDEN_PRESPIN 0
+#define LSVD_ROTOR_KIND_CAUSAL_ANTISPIN 1
+#define LSVD_ROTOR_KIND_CROSS_PHASE_YINYANG 2
+#define LSVD_ROTOR_KIND_PHASE_CONJUGATE 3
+#define LSVD_ROTOR_KIND_BOTTLENECK 4
+#define LSVD_ROTOR_KIND_PHASE_JUMP 5
+#define LSVD_ROTOR_KIND_UNWRAP 6
+#define LSVD_ROTOR_KIND_DIRECTIONAL 7
+#define LSVD_ROTOR_KIND_SURGERY 8
+
+/* Replaces HardwareSchedule::from_real_phaseflow + to_json_string
+ * (src/lie_svd_compiler.rs:59-88, :213-265): layer = pass, theta =
+ * (theta_l + theta_r) / 2, phi_l = phi_r = 0, source "real_phaseflow", kind
+ * by name (:268-280), no diagonal_signs.  JSON out as lsvd_schedule_from_*. */
+LSVD_API lsvd_status lsvd_schedule_from_real_phaseflow(const lsvd_mzi_phase* events, int64_t count,
+                                                       int64_t channels, int32_t target, char* json,
+                                                       int64_t cap, int64_t* len);
+
+/* ---------------------------------------- binary phase-schedule frame ---- */
+/* The phase-schedule-v1 data model (src/lie_svd_compiler.rs:27-57) as one
+ * little-endian frame, for targets that take fixed records (the reference's
+ * intended CBOR / FPGA-table / MZI-frame mappings, no counterpart of its
+ * own): header, total_events records, n_signs doubles (diagonal_signs),
+ * then, with LSVD_SCHED_ENERGY, two doubles per event (energy_before,
+ * energy_after; NaN = absent).  Source and kind are codes into the fixed
+ * name tables LSVD_SCHED_SOURCE_* / LSVD_SCHED_KIND_* (kinds 0..8 are the
+ * LSVD_ROTOR_KIND_* names, 9 complex_golden_prespin, 10
+ * complex_diagonal_phase, 11 givens_elimination, 12 jacobi_rotation).
+ * With LSVD_SCHED_CANONICAL the JSON order is the records stably sorted by
+ * (layer, j, i) -- the (round, i, j) order of the rotors they come from, whose
+ * pair the record stores as (i, j) = (rotor j, rotor i); a device-written
+ * stream carries its events in the order the sweeps produced them. */
+#define LSVD_SCHED_MAGIC "PSCHEDv1"
+#define LSVD_SCHED_CANONICAL 0x1u
+#define LSVD_SCHED_ENERGY 0x2u
+#define LSVD_SCHED_SOURCE_REAL_PHASEFLOW 0
+#define LSVD_SCHED_SOURCE_COMPLEX_PHASEFLOW 1
+#define LSVD_SCHED_SOURCE_ORTHOGONAL_GIVENS 2
+#define LSVD_SCHED_SOURCE_GPU_JACOBI 3
+#define LSVD_SCHED_KIND_GIVENS_ELIMINATION 11
+#define LSVD_SCHED_KIND_JACOBI_ROTATION 12
+
+typedef struct lsvd_schedule_header {
+    char magic[8];         /* LSVD_SCHED_MAGIC, no NUL */
+    uint32_t header_bytes; /* sizeof(lsvd_schedule_header) = 64 */
+    uint32_t record_bytes; /* sizeof(lsvd_schedule_record) = 56 */
+    uint32_t target;       /* 0 mzi_mesh, 1 fpga_rotor_mesh */
+    uint32_t flags;        /* LSVD_SCHED_* */
+    int64_t channels;
+    int64_t total_events;
+    int64_t n_signs;
+    int64_t reserved[2];
+} lsvd_schedule_header;
+
+typedef struct lsvd_schedule_record {
+    uint32_t layer;
+    uint16_t i;
+    uint16_t j;
+    double phi_l;
+    double phi_r;
+    double theta;
+    double theta_l;
+    double theta_r;
+    uint8_t source;
+    uint8_t kind;
+    uint16_t reserved0;
+    uint32_t reserved1;
+} lsvd_schedule_record;
+
+/* Binary frame of a rotor stream: the events of lsvd_schedule_from_rotors
+ * (same convention, diagonal_signs all +1) in stream order, with
+ * LSVD_SCHED_CANONICAL.  With LSVD_DEVICE_POINTERS `rotors` and `out` are
+ * device memory and one kernel writes the whole frame on the context's
+ * stream (synchronous unless LSVD_ASYNC; a bad rotor -- i >= j or
+ * j >= channels -- is then reported by LSVD_BAD_ARGUMENT only when not
+ * asynchronous); otherwise both are host memory and ctx may be NULL.
+ * *len (host) receives the frame's size in bytes; cap below it returns
+ * LSVD_ROTOR_OVERFLOW with nothing written (out = NULL to size). */
+LSVD_API lsvd_status lsvd_schedule_binary_from_rotors(lsvd_context* ctx, const lsvd_rotor* rotors,
+                                                      int64_t count, int64_t channels, int32_t target,
+                                                      void* out, int64_t cap, int64_t* len,
+                                                      uint32_t flags);
+
+/* Binary frame of lsvd_schedule_from_real_phaseflow's schedule (host). */
+LSVD_API lsvd_status lsvd_schedule_binary_from_real_phaseflow(const lsvd_mzi_phase* events,
+                                                              int64_t count, int64_t channels,
+                                                              int32_t target, void* out, int64_t cap,
+                                                              int64_t* len);
+
+/* The phase-schedule-v1 JSON text of a binary frame (host), byte-identical
+ * to the JSON entry that describes the same schedule.  A malformed frame
+ * (magic, sizes, codes, length) returns LSVD_BAD_ARGUMENT. */
+LSVD_API lsvd_status lsvd_schedule_binary_to_json(const void* frame, int64_t bytes, char* json,
+                                                  int64_t cap, int64_t* len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,20 @@ class Rotor(C.Structure):
 DIAG_DTYPE = [("rel_recon", "<f8"), ("orth_u", "<f8"), ("orth_v", "<f8"), ("ns_iters", "<i4"),
               ("jacobi_sweeps", "<i4"), ("rotations", "<i8"), ("flags", "<i4"), ("route", "<i4")]
 ROTOR_DTYPE = [("i", "<u2"), ("j", "<u2"), ("round", "<u4"), ("theta", "<f8")]
+# lsvd_mzi_phase (MziPhase of the real PhaseFlow route) and the binary
+# phase-schedule frame's header and record
+MZI_PHASE_DTYPE = [("pass", "<i8"), ("i", "<i8"), ("j", "<i8"), ("theta_l", "<f8"), ("theta_r", "<f8"),
+                   ("kind", "<i4"), ("pad_", "<i4")]
+SCHED_HEADER_DTYPE = [("magic", "S8"), ("header_bytes", "<u4"), ("record_bytes", "<u4"), ("target", "<u4"),
+                      ("flags", "<u4"), ("channels", "<i8"), ("total_events", "<i8"), ("n_signs", "<i8"),
+                      ("reserved", "<i8", (2,))]
+SCHED_RECORD_DTYPE = [("layer", "<u4"), ("i", "<u2"), ("j", "<u2"), ("phi_l", "<f8"), ("phi_r", "<f8"),
+                      ("theta", "<f8"), ("theta_l", "<f8"), ("theta_r", "<f8"), ("source", "u1"), ("kind", "u1"),
+                      ("reserved0", "<u2"), ("reserved1", "<u4")]
+PHASE_ROTOR_KINDS = ("golden_prespin", "causal_antispin", "cross_phase_yinyang", "phase_conjugate",
+                     "bottleneck", "phase_jump", "unwrap", "directional", "surgery")
+SCHED_CANONICAL = 0x1
+SCHED_ENERGY = 0x2
 
 
 class JointParams(C.Structure):
@@ -123,6 +137,11 @@ SIGNATURES = {
                                    C.c_double, P, U32]),
     "lsvd_schedule_from_orthogonal": (C.c_int, [I64, P, C.c_int32, P, I64, C.POINTER(I64)]),
     "lsvd_schedule_from_rotors": (C.c_int, [P, I64, I64, C.c_int32, P, I64, C.POINTER(I64)]),
+    "lsvd_schedule_from_real_phaseflow": (C.c_int, [P, I64, I64, C.c_int32, P, I64, C.POINTER(I64)]),
+    "lsvd_schedule_binary_from_rotors": (C.c_int, [P, P, I64, I64, C.c_int32, P, I64, C.POINTER(I64),
+                                                   C.c_uint32]),
+    "lsvd_schedule_binary_from_real_phaseflow": (C.c_int, [P, I64, I64, C.c_int32, P, I64, C.POINTER(I64)]),
+    "lsvd_schedule_binary_to_json": (C.c_int, [P, I64, P, I64, C.POINTER(I64)]),
 }
 
 OPTIONAL_SIGNATURES: dict = {}

@@ -514,6 +514,86 @@ class HardwareSchedule:
         return _json_call(lib.lsvd_schedule_from_rotors, _ptr(r) if r.size else None, r.size,
                           channels, TARGETS[target])
 
+    @staticmethod
+    def _mzi_events(events):
+        """MziPhase events (src/lie_svd_phaseflow.rs:202-209) as a structured
+        array: either already of MZI_PHASE_DTYPE, or (pass, i, j, theta_l,
+        theta_r, kind) tuples with kind a PhaseRotorKind name or index."""
+        if isinstance(events, np.ndarray) and events.dtype == np.dtype(L.MZI_PHASE_DTYPE):
+            return np.ascontiguousarray(events)
+        ev = np.zeros(len(events), dtype=L.MZI_PHASE_DTYPE)
+        for k, (ps, i, j, tl, tr, kind) in enumerate(events):
+            kind = L.PHASE_ROTOR_KINDS.index(kind) if isinstance(kind, str) else int(kind)
+            ev[k] = (ps, i, j, tl, tr, kind, 0)
+        return ev
+
+    @staticmethod
+    def from_real_phaseflow_json(events, channels: int, target: str = "mzi_mesh") -> str:
+        """``HardwareSchedule::from_real_phaseflow(..).to_json_string()``
+        (src/lie_svd_compiler.rs:59-88, :213-265)."""
+        ev = HardwareSchedule._mzi_events(events)
+        return _json_call(L.load().lsvd_schedule_from_real_phaseflow, _ptr(ev) if ev.size else None, ev.size,
+                          channels, TARGETS[target])
+
+    @staticmethod
+    def _frame_call(fn, *args, tail=()) -> bytes:
+        n = C.c_int64(0)
+        st = fn(*args, None, 0, C.byref(n), *tail)
+        if st != L.OK:
+            raise L.LsvdError(st, "schedule frame sizing failed")
+        buf = np.empty(n.value, dtype=np.uint8)
+        st = fn(*args, _ptr(buf), n.value, C.byref(n), *tail)
+        if st != L.OK:
+            raise L.LsvdError(st, "schedule frame encoding failed")
+        return buf.tobytes()
+
+    @staticmethod
+    def from_real_phaseflow_binary(events, channels: int, target: str = "mzi_mesh") -> bytes:
+        """Binary phase-schedule frame of ``from_real_phaseflow``'s schedule."""
+        ev = HardwareSchedule._mzi_events(events)
+        return HardwareSchedule._frame_call(L.load().lsvd_schedule_binary_from_real_phaseflow,
+                                            _ptr(ev) if ev.size else None, ev.size, channels, TARGETS[target])
+
+    @staticmethod
+    def from_rotor_stream_binary(rotors, channels: int, target: str = "mzi_mesh", ctx=None):
+        """Binary phase-schedule frame of a rotor stream.  A CUDA tensor of
+        16-byte rotors (any dtype viewing the lsvd_rotor records, e.g. the
+        stream buffer of ``svd_batched_stream``) is encoded on the device and
+        returned as a CUDA uint8 tensor; a numpy stream on the host, as bytes."""
+        lib = L.load()
+        if _is_torch(rotors) and rotors.is_cuda:
+            import torch
+            rb = rotors.contiguous().view(torch.uint8)
+            if rb.numel() % 16:
+                raise L.LsvdError(L.BAD_ARGUMENT, "rotor stream is not a whole number of 16-byte records")
+            count = rb.numel() // 16
+            ctx = ctx or default_context(rotors.device.index or 0)
+            torch.cuda.current_stream(rotors.device).synchronize()
+            n = C.c_int64(0)
+            st = lib.lsvd_schedule_binary_from_rotors(ctx.handle, C.c_void_p(rb.data_ptr()), count, channels,
+                                                      TARGETS[target], None, 0, C.byref(n), L.DEVICE_POINTERS)
+            if st != L.OK:
+                raise L.LsvdError(st, "schedule frame sizing failed")
+            out = torch.empty(n.value, dtype=torch.uint8, device=rotors.device)
+            st = lib.lsvd_schedule_binary_from_rotors(ctx.handle, C.c_void_p(rb.data_ptr()), count, channels,
+                                                      TARGETS[target], C.c_void_p(out.data_ptr()), n.value,
+                                                      C.byref(n), L.DEVICE_POINTERS)
+            _check(lib, ctx.handle, st, "lsvd_schedule_binary_from_rotors")
+            return out
+        r = np.ascontiguousarray(rotors, dtype=L.ROTOR_DTYPE)
+        return HardwareSchedule._frame_call(lib.lsvd_schedule_binary_from_rotors, None, _ptr(r) if r.size else None,
+                                            r.size, channels, TARGETS[target], tail=(0,))
+
+    @staticmethod
+    def binary_to_json(frame) -> str:
+        """phase-schedule-v1 JSON text of a binary frame (bytes, numpy or a
+        CUDA uint8 tensor, copied to the host first)."""
+        if _is_torch(frame):
+            frame = frame.cpu().numpy()
+        buf = np.frombuffer(bytes(frame), dtype=np.uint8) if not isinstance(frame, np.ndarray) else frame
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        return _json_call(L.load().lsvd_schedule_binary_to_json, _ptr(buf), buf.size)
+
 
 @dataclass
 class JointDiagonalizationParams:

@@ -39,8 +39,18 @@ def _deps_mtime() -> float:
     return max(os.path.getmtime(f) for f in files)
 
 
-def _compile(src: str, verbose: bool, extra: list[str]) -> str:
+def _headers_mtime() -> float:
+    files = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+        glob.glob(os.path.join(INCLUDE, "*.h"))
+    return max(os.path.getmtime(f) for f in files)
+
+
+def _compile(src: str, verbose: bool, extra: list[str], reuse_after: float | None = None) -> str:
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    # an object newer than its source and every header is current
+    if reuse_after is not None and os.path.exists(obj) and \
+            os.path.getmtime(obj) >= max(os.path.getmtime(src), reuse_after):
+        return obj
     cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", src, "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
@@ -62,7 +72,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         return LIB
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose or ptxas_verbose, extra), srcs))
+        reuse = None if (force or ptxas_verbose) else _headers_mtime()
+        objs = list(ex.map(lambda s: _compile(s, verbose or ptxas_verbose, extra, reuse), srcs))
     cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -377,32 +377,49 @@ __global__ void offnorm_final_kernel(const double* __restrict__ part, int nparts
     }
 }
 
+// Round-robin slot k (0..31) of round `round` over 64 indices: the circle
+// method of src/lie_svd_joint.rs:524-539 (index 63 fixed in slot 0).
+__device__ __forceinline__ void rr_slot(int round, int k, int& p, int& q) {
+    if (k == 0) {
+        p = PW - 1;
+        q = round;
+    } else {
+        p = round + k;
+        p -= p >= PW - 1 ? PW - 1 : 0;
+        q = round - k;
+        q += q < 0 ? PW - 1 : 0;
+    }
+}
+
 // Two-sided route (1024 threads: the 63 rounds of a block sweep are the
-// critical path of every layer, so each round's 32 x 32 two-sided 2 x 2
-// updates take one per thread): gathers the 64 x 64 diagonal block of block
-// pair blockIdx.x from P, diagonalises it (rotations of |a_pq| > tau, the
-// reference rotating every |a_pq| >= 1e-300, src/lie_svd_small.rs:233-235),
-// and writes R / skip like solve_kernel.
+// critical path of every layer): gathers the 64 x 64 diagonal block M of
+// block pair blockIdx.x from P, diagonalises it (rotations of |a_pq| > tau,
+// the reference rotating every |a_pq| >= 1e-300, src/lie_svd_small.rs:
+// 233-235) and writes R / skip like solve_kernel.  Per round, warp 0
+// computes the 32 rotations (lane k <-> slot k); threads t < 528 update one
+// 2 x 2 block (slot a <= slot b) of the symmetric M as J_a^T M_ab J_b and
+// store it and its transpose; R never touches shared memory: thread
+// (warp w, lane k) keeps R's rows w and w + 32 at the two columns of slot k
+// in registers, rotates them, and hands them to the slots they occupy in the
+// next round by one shuffle each way (slot k's first index moves to slot
+// k - 1, its second to slot k + 1; the ends turn around).  After the 63
+// rounds of a sweep every column is back in its round-0 slot.
 __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__ P, int64_t ldp, int nb, int layer,
                                                      double* __restrict__ Rg, int* __restrict__ skip,
                                                      SweepState* __restrict__ stt, double tau, int inner_max) {
     if (stt->converged) return;
     extern __shared__ __align__(16) double ssmem[];
     double* Ms = ssmem;
-    double* Rs = ssmem + PW * MLD;
     __shared__ double cs[32], sn[32];
-    __shared__ int pa[32], qa[32];
     __shared__ double red[32];
-    __shared__ int s_cnt, s_flag;
-    const int pair = blockIdx.x, tid = threadIdx.x;
+    __shared__ int s_flag;
+    const int pair = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int Pb, Qb;
     block_pair(nb, layer, pair, Pb, Qb);
     for (int e = tid; e < PW * PW; e += 1024) {
         const int i = e >> 6, j = e & 63;
         Ms[i * MLD + j] = P[int64_t(pair_index(i, Pb, Qb)) * ldp + pair_index(j, Pb, Qb)];
-        Rs[i * MLD + j] = i == j ? 1.0 : 0.0;
     }
-    if (tid == 0) s_cnt = 0;
     __syncthreads();
     double off = 0.0;
     for (int e = tid; e < PW * PW; e += 1024) {
@@ -414,15 +431,107 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
         if (tid == 0) skip[pair] = 1;
         return;
     }
-    const int sw = inner_jacobi<1024>(
-        Ms, Rs, inner_max, [&](double, double, double apq) { return fabs(apq) > tau; }, cs, sn, pa, qa, &s_flag,
-        &s_cnt);
+    // this thread's block (ka, kb), ka <= kb, of the 32 x 32 slot triangle
+    int ka = 0, kb = 0;
+    const bool upd = tid < 32 * 33 / 2;
+    if (upd) {
+        int rem = tid;
+        while (rem >= 32 - ka) {
+            rem -= 32 - ka;
+            ++ka;
+        }
+        kb = ka + rem;
+    }
+    // R rows warp and warp + 32 at the round-0 columns of slot `lane`
+    int c0p, c0q;
+    rr_slot(0, lane, c0p, c0q);
+    double rp0 = warp == c0p ? 1.0 : 0.0, rq0 = warp == c0q ? 1.0 : 0.0;
+    double rp1 = warp + 32 == c0p ? 1.0 : 0.0, rq1 = warp + 32 == c0q ? 1.0 : 0.0;
+    int cnt = 0, sweep = 0;
+    for (; sweep < inner_max; ++sweep) {
+        if (tid == 0) s_flag = 0;
+        __syncthreads();
+        for (int round = 0; round < PW - 1; ++round) {
+            if (warp == 0) {
+                int p, qq;
+                rr_slot(round, lane, p, qq);
+                const double app = Ms[p * MLD + p], aqq = Ms[qq * MLD + qq], apq = Ms[p * MLD + qq];
+                double c = 1.0, s = 0.0;
+                const bool rot = apq != 0.0 && fabs(apq) > tau;
+                if (rot) {
+                    // Rutishauser's tangent (src/lie_svd_small.rs:235-242)
+                    const double zeta = (aqq - app) / (2.0 * apq);
+                    const double t = fabs(zeta) > 1e150
+                                         ? 0.5 / zeta
+                                         : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    c = rsqrt(1.0 + t * t);
+                    s = t * c;
+                }
+                const unsigned msk = __ballot_sync(0xffffffffu, rot);
+                if (lane == 0 && msk) {
+                    cnt += __popc(msk);
+                    s_flag = 1;
+                }
+                cs[lane] = c;
+                sn[lane] = s;
+            }
+            __syncthreads();
+            if (upd) {
+                const double ca = cs[ka], sa = sn[ka], cb = cs[kb], sb = sn[kb];
+                if (sa != 0.0 || sb != 0.0) {
+                    int ra, rb, ca_, cb_;
+                    rr_slot(round, ka, ra, rb);
+                    rr_slot(round, kb, ca_, cb_);
+                    const double x = Ms[ra * MLD + ca_], y = Ms[ra * MLD + cb_];
+                    const double z = Ms[rb * MLD + ca_], w = Ms[rb * MLD + cb_];
+                    const double x1 = cb * x - sb * y, y1 = sb * x + cb * y;
+                    const double z1 = cb * z - sb * w, w1 = sb * z + cb * w;
+                    const double x2 = ca * x1 - sa * z1, w2 = sa * y1 + ca * w1;
+                    double y2 = ca * y1 - sa * w1, z2 = sa * x1 + ca * z1;
+                    if (ka == kb) y2 = z2 = 0.0;  // the pair this rotation annihilates
+                    Ms[ra * MLD + ca_] = x2;
+                    Ms[ra * MLD + cb_] = y2;
+                    Ms[rb * MLD + ca_] = z2;
+                    Ms[rb * MLD + cb_] = w2;
+                    if (ka != kb) {
+                        Ms[ca_ * MLD + ra] = x2;
+                        Ms[cb_ * MLD + ra] = y2;
+                        Ms[ca_ * MLD + rb] = z2;
+                        Ms[cb_ * MLD + rb] = w2;
+                    }
+                }
+            }
+            {
+                // R <- R J on the registers, then the move to the next round's slots
+                const double c = cs[lane], s = sn[lane];
+                const double u0 = c * rp0 - s * rq0, v0 = s * rp0 + c * rq0;
+                const double u1 = c * rp1 - s * rq1, v1 = s * rp1 + c * rq1;
+                const double dp0 = __shfl_down_sync(0xffffffffu, u0, 1), dp1 = __shfl_down_sync(0xffffffffu, u1, 1);
+                const double uq0 = __shfl_up_sync(0xffffffffu, v0, 1), uq1 = __shfl_up_sync(0xffffffffu, v1, 1);
+                if (lane == 0) {
+                    rp0 = u0, rp1 = u1, rq0 = dp0, rq1 = dp1;
+                } else if (lane == 31) {
+                    rp0 = v0, rp1 = v1, rq0 = uq0, rq1 = uq1;
+                } else {
+                    rp0 = dp0, rp1 = dp1, rq0 = uq0, rq1 = uq1;
+                }
+            }
+            __syncthreads();
+        }
+        const int any = s_flag;
+        __syncthreads();
+        if (!any) break;
+    }
+    const int sw = sweep == inner_max ? inner_max + 1 : sweep + 1;
     double* R = Rg + int64_t(pair) * (PW * PW);
-    for (int e = tid; e < PW * PW; e += 1024) R[e] = Rs[(e >> 6) * MLD + (e & 63)];
+    R[warp * PW + c0p] = rp0;
+    R[warp * PW + c0q] = rq0;
+    R[(warp + 32) * PW + c0p] = rp1;
+    R[(warp + 32) * PW + c0q] = rq1;
     if (tid == 0) {
         skip[pair] = 0;
         stt->rotated = 1;
-        atomicAdd(&stt->rotations, (unsigned long long)s_cnt);
+        atomicAdd(&stt->rotations, (unsigned long long)cnt);
         if (sw > inner_max) atomicAdd(&stt->inner_cap, 1);
     }
 }
@@ -832,7 +941,8 @@ __global__ void transpose_kernel(int rows, int cols, const double* in, int64_t l
 
 constexpr int kApplySmem = 3 * PW * XLD * 8;  // R + two stages: 104448 bytes
 constexpr int kGramSmem = 3 * PW * GLD * 8;   // three stages: 55296 bytes
-constexpr int kSolveSmem = 2 * PW * MLD * 8;  // M and R: 66560 bytes
+constexpr int kSolveSmem = 2 * PW * MLD * 8;  // M and R: 66560 bytes (solve_kernel)
+constexpr int kSolve2Smem = PW * MLD * 8;    // M: 33280 bytes
 constexpr int kTwoSmem = 3 * PW * XLD * 8;    // P_ab / T, R_a, R_b: 104448 bytes
 
 struct EventTimer {
@@ -994,7 +1104,7 @@ static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, 
     double* offpart = reinterpret_cast<double*>(p);  // 256 partial sums of the off-norm test
     cudaError_t e = cudaMemsetAsync(stt, 0, sizeof(SweepState), st);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(solve2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(solve2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolve2Smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(twoside_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTwoSmem);
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: sweep setup");
     if (!ctx->side_stream && (e = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking)) != cudaSuccess)
@@ -1023,7 +1133,7 @@ static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, 
         const int b = layer & 1;
         // the buffers of parity b were last read by V's update two layers back
         if (layer >= 2) cudaStreamWaitEvent(st, evs[2 + b], 0);
-        solve2_kernel<<<npairs, 1024, kSolveSmem, st>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt, tau, inner_max);
+        solve2_kernel<<<npairs, 1024, kSolve2Smem, st>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt, tau, inner_max);
         cudaEventRecord(evs[0], st);
         cudaStreamWaitEvent(sv, evs[0], 0);
         apply_kernel<<<dim3(npairs, napply), 256, kApplySmem, sv>>>(Vc, npad, nb, layer, rows, Rg2[b], skip2[b], stt);

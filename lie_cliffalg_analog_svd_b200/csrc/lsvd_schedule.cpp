@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "lsvd.h"
+#include "lsvd_schedule_frame.h"
 
 namespace {
 
@@ -18,6 +19,8 @@ struct Event {
     double phi_l, phi_r, theta, theta_l, theta_r;
     const char* source;
     const char* kind;
+    bool has_before = false, has_after = false;  // Option<f64> energy_before / energy_after
+    double energy_before = 0.0, energy_after = 0.0;
 };
 
 // Rust `{:.17e}`: 17 fractional digits, exponent without '+' or zero padding.
@@ -47,6 +50,19 @@ std::string fmt_display(double x) {
 
 const char* target_name(int target) { return target == 1 ? "fpga_rotor_mesh" : "mzi_mesh"; }
 
+// Name tables of the binary frame's codes: sources as HardwareSchedule's
+// constructors write them, kinds as real_kind / complex_kind
+// (src/lie_svd_compiler.rs:268-287) and the two solver-side kinds.
+constexpr const char* kSources[] = {"real_phaseflow", "complex_phaseflow", "orthogonal_givens", "gpu_jacobi"};
+constexpr const char* kKinds[] = {"golden_prespin", "causal_antispin", "cross_phase_yinyang",
+                                  "phase_conjugate", "bottleneck", "phase_jump",
+                                  "unwrap", "directional", "surgery",
+                                  "complex_golden_prespin", "complex_diagonal_phase", "givens_elimination",
+                                  "jacobi_rotation"};
+constexpr int kNumSources = int(sizeof(kSources) / sizeof(kSources[0]));
+constexpr int kNumKinds = int(sizeof(kKinds) / sizeof(kKinds[0]));
+constexpr int kNumRealKinds = 9;
+
 // to_json_string, src/lie_svd_compiler.rs:213-265.
 std::string to_json(int target, int64_t channels, const std::vector<Event>& ev,
                     const std::vector<double>& signs) {
@@ -62,7 +78,10 @@ std::string to_json(int target, int64_t channels, const std::vector<Event>& ev,
                ", \"j\": " + std::to_string(e.j) + ", \"phi_l\": " + fmt_e17(e.phi_l) +
                ", \"phi_r\": " + fmt_e17(e.phi_r) + ", \"theta\": " + fmt_e17(e.theta) +
                ", \"theta_l\": " + fmt_e17(e.theta_l) + ", \"theta_r\": " + fmt_e17(e.theta_r) +
-               ", \"source\": \"" + e.source + "\", \"kind\": \"" + e.kind + "\"}";
+               ", \"source\": \"" + e.source + "\", \"kind\": \"" + e.kind + "\"";
+        if (e.has_before) out += ", \"energy_before\": " + fmt_e17(e.energy_before);
+        if (e.has_after) out += ", \"energy_after\": " + fmt_e17(e.energy_after);
+        out += "}";
         if (k + 1 != ev.size()) out += ",";
         out += "\n";
     }
@@ -157,4 +176,140 @@ extern "C" LSVD_API lsvd_status lsvd_schedule_from_rotors(const lsvd_rotor* roto
                            -r.theta, -r.theta, "gpu_jacobi", "jacobi_rotation"});
     std::vector<double> signs(static_cast<size_t>(channels), 1.0);
     return emit(to_json(target, channels, ev, signs), json, cap, len);
+}
+
+namespace {
+
+bool phaseflow_ok(const lsvd_mzi_phase* events, int64_t count, int64_t channels, int32_t target) {
+    if (count < 0 || channels < 0 || (count > 0 && !events) || (target != 0 && target != 1)) return false;
+    for (int64_t k = 0; k < count; ++k)
+        if (events[k].kind < 0 || events[k].kind >= kNumRealKinds || events[k].pass < 0 || events[k].i < 0 ||
+            events[k].j < 0)
+            return false;
+    return true;
+}
+
+// Copies a finished frame (or reports its size): *len = bytes; cap too small
+// writes nothing.
+lsvd_status emit_frame(const std::vector<unsigned char>& f, void* out, int64_t cap, int64_t* len) {
+    if (len) *len = int64_t(f.size());
+    if (!out) return LSVD_OK;
+    if (cap < int64_t(f.size())) return LSVD_ROTOR_OVERFLOW;
+    std::memcpy(out, f.data(), f.size());
+    return LSVD_OK;
+}
+
+std::vector<unsigned char> build_frame(int32_t target, uint32_t flags, int64_t channels,
+                                       const std::vector<lsvd_schedule_record>& rec,
+                                       const std::vector<double>& signs) {
+    std::vector<unsigned char> f(size_t(lsvd::sched::frame_bytes(int64_t(rec.size()), int64_t(signs.size()), false)));
+    const lsvd_schedule_header h =
+        lsvd::sched::make_header(target, flags, channels, int64_t(rec.size()), int64_t(signs.size()));
+    std::memcpy(f.data(), &h, sizeof(h));
+    if (!rec.empty()) std::memcpy(f.data() + sizeof(h), rec.data(), rec.size() * sizeof(lsvd_schedule_record));
+    if (!signs.empty())
+        std::memcpy(f.data() + sizeof(h) + rec.size() * sizeof(lsvd_schedule_record), signs.data(),
+                    signs.size() * 8);
+    return f;
+}
+
+}  // namespace
+
+// HardwareSchedule::from_real_phaseflow + to_json_string
+// (src/lie_svd_compiler.rs:59-88, :213-265).
+extern "C" LSVD_API lsvd_status lsvd_schedule_from_real_phaseflow(const lsvd_mzi_phase* events, int64_t count,
+                                                                  int64_t channels, int32_t target, char* json,
+                                                                  int64_t cap, int64_t* len) {
+    if (!phaseflow_ok(events, count, channels, target)) return LSVD_BAD_ARGUMENT;
+    std::vector<Event> ev;
+    ev.reserve(size_t(count));
+    for (int64_t k = 0; k < count; ++k) {
+        const lsvd_mzi_phase& e = events[k];
+        ev.push_back(Event{e.pass, e.i, e.j, 0.0, 0.0, 0.5 * (e.theta_l + e.theta_r), e.theta_l, e.theta_r,
+                           kSources[LSVD_SCHED_SOURCE_REAL_PHASEFLOW], kKinds[e.kind]});
+    }
+    return emit(to_json(target, channels, ev, {}), json, cap, len);
+}
+
+extern "C" LSVD_API lsvd_status lsvd_schedule_binary_from_real_phaseflow(const lsvd_mzi_phase* events,
+                                                                         int64_t count, int64_t channels,
+                                                                         int32_t target, void* out, int64_t cap,
+                                                                         int64_t* len) {
+    if (!phaseflow_ok(events, count, channels, target)) return LSVD_BAD_ARGUMENT;
+    std::vector<lsvd_schedule_record> rec(static_cast<size_t>(count));
+    for (int64_t k = 0; k < count; ++k) {
+        const lsvd_mzi_phase& e = events[k];
+        if (e.pass > 0xffffffffLL || e.i > lsvd::sched::kMaxChannels || e.j > lsvd::sched::kMaxChannels)
+            return LSVD_UNSUPPORTED;
+        lsvd_schedule_record& r = rec[size_t(k)];
+        std::memset(&r, 0, sizeof(r));
+        r.layer = uint32_t(e.pass);
+        r.i = uint16_t(e.i);
+        r.j = uint16_t(e.j);
+        r.theta = 0.5 * (e.theta_l + e.theta_r);
+        r.theta_l = e.theta_l;
+        r.theta_r = e.theta_r;
+        r.source = uint8_t(LSVD_SCHED_SOURCE_REAL_PHASEFLOW);
+        r.kind = uint8_t(e.kind);
+    }
+    return emit_frame(build_frame(target, 0u, channels, rec, {}), out, cap, len);
+}
+
+// Host half of lsvd_schedule_binary_from_rotors (the device half is in
+// lsvd_schedule_dev.cu).
+lsvd_status lsvd_schedule_binary_rotors_host(const lsvd_rotor* rotors, int64_t count, int64_t channels,
+                                             int32_t target, void* out, int64_t cap, int64_t* len) {
+    std::vector<lsvd_schedule_record> rec(static_cast<size_t>(count));
+    for (int64_t k = 0; k < count; ++k) {
+        if (!lsvd::sched::rotor_ok(rotors[k], channels)) return LSVD_BAD_ARGUMENT;
+        rec[size_t(k)] = lsvd::sched::rotor_record(rotors[k]);
+    }
+    const std::vector<double> signs(size_t(channels), 1.0);
+    return emit_frame(build_frame(target, LSVD_SCHED_CANONICAL, channels, rec, signs), out, cap, len);
+}
+
+extern "C" LSVD_API lsvd_status lsvd_schedule_binary_to_json(const void* frame, int64_t bytes, char* json,
+                                                             int64_t cap, int64_t* len) {
+    const int64_t hb = int64_t(sizeof(lsvd_schedule_header));
+    if (!frame || bytes < hb) return LSVD_BAD_ARGUMENT;
+    lsvd_schedule_header h;
+    std::memcpy(&h, frame, sizeof(h));
+    if (std::memcmp(h.magic, LSVD_SCHED_MAGIC, 8) != 0 || h.header_bytes != sizeof(lsvd_schedule_header) ||
+        h.record_bytes != sizeof(lsvd_schedule_record) || h.target > 1 ||
+        (h.flags & ~(LSVD_SCHED_CANONICAL | LSVD_SCHED_ENERGY)) != 0 || h.channels < 0 || h.total_events < 0 ||
+        h.n_signs < 0 || h.total_events > bytes || h.n_signs > bytes)
+        return LSVD_BAD_ARGUMENT;
+    const bool energy = (h.flags & LSVD_SCHED_ENERGY) != 0;
+    if (lsvd::sched::frame_bytes(h.total_events, h.n_signs, energy) != bytes) return LSVD_BAD_ARGUMENT;
+    const unsigned char* base = static_cast<const unsigned char*>(frame);
+    const unsigned char* rp = base + hb;
+    const unsigned char* sp = rp + h.total_events * int64_t(sizeof(lsvd_schedule_record));
+    const unsigned char* ep = sp + h.n_signs * 8;
+    std::vector<Event> ev;
+    ev.reserve(size_t(h.total_events));
+    for (int64_t k = 0; k < h.total_events; ++k) {
+        lsvd_schedule_record r;
+        std::memcpy(&r, rp + k * int64_t(sizeof(r)), sizeof(r));
+        if (r.source >= kNumSources || r.kind >= kNumKinds) return LSVD_BAD_ARGUMENT;
+        Event e{int64_t(r.layer), int64_t(r.i), int64_t(r.j), r.phi_l, r.phi_r, r.theta, r.theta_l, r.theta_r,
+                kSources[r.source], kKinds[r.kind]};
+        if (energy) {
+            double eb[2];
+            std::memcpy(eb, ep + k * 16, 16);
+            e.has_before = !std::isnan(eb[0]);
+            e.has_after = !std::isnan(eb[1]);
+            e.energy_before = eb[0];
+            e.energy_after = eb[1];
+        }
+        ev.push_back(e);
+    }
+    if (h.flags & LSVD_SCHED_CANONICAL)
+        std::stable_sort(ev.begin(), ev.end(), [](const Event& a, const Event& b) {
+            if (a.layer != b.layer) return a.layer < b.layer;
+            if (a.j != b.j) return a.j < b.j;
+            return a.i < b.i;
+        });
+    std::vector<double> signs(size_t(h.n_signs));
+    if (h.n_signs) std::memcpy(signs.data(), sp, size_t(h.n_signs) * 8);
+    return emit(to_json(int(h.target), h.channels, ev, signs), json, cap, len);
 }

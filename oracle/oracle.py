@@ -348,6 +348,16 @@ class HardwareSchedule:
                for k in range(cnt)]
         return HardwareSchedule(target, d, evs, [float(x) for x in sg[:d]])
 
+    @staticmethod
+    def from_real_phaseflow(events, channels: int, target: str = "mzi_mesh") -> "HardwareSchedule":
+        """``from_real_phaseflow`` (src/lie_svd_compiler.rs:59-88): events are
+        MziPhase tuples (pass, i, j, theta_l, theta_r, kind name)."""
+        evs = [HardwarePhaseEvent(layer=int(ps), i=int(i), j=int(j), phi_l=0.0, phi_r=0.0,
+                                  theta=0.5 * (float(tl) + float(tr)), theta_l=float(tl), theta_r=float(tr),
+                                  source="real_phaseflow", kind=str(kind))
+               for ps, i, j, tl, tr, kind in events]
+        return HardwareSchedule(target, channels, evs, [])
+
     def total_events(self) -> int:
         return len(self.events)
 

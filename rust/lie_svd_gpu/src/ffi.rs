@@ -117,6 +117,49 @@ pub struct LsvdPolarInfo {
     pub pad_: i32,
 }
 
+#[repr(C)]
+#[derive(Default, Clone, Copy, Debug)]
+pub struct LsvdMziPhase {
+    pub pass: i64,
+    pub i: i64,
+    pub j: i64,
+    pub theta_l: f64,
+    pub theta_r: f64,
+    pub kind: i32,
+    pub pad_: i32,
+}
+
+#[repr(C)]
+#[derive(Default, Clone, Copy, Debug)]
+pub struct LsvdScheduleHeader {
+    pub magic: [u8; 8],
+    pub header_bytes: u32,
+    pub record_bytes: u32,
+    pub target: u32,
+    pub flags: u32,
+    pub channels: i64,
+    pub total_events: i64,
+    pub n_signs: i64,
+    pub reserved: [i64; 2],
+}
+
+#[repr(C)]
+#[derive(Default, Clone, Copy, Debug)]
+pub struct LsvdScheduleRecord {
+    pub layer: u32,
+    pub i: u16,
+    pub j: u16,
+    pub phi_l: f64,
+    pub phi_r: f64,
+    pub theta: f64,
+    pub theta_l: f64,
+    pub theta_r: f64,
+    pub source: u8,
+    pub kind: u8,
+    pub reserved0: u16,
+    pub reserved1: u32,
+}
+
 #[link(name = "lsvd_b200")]
 extern "C" {
     pub fn lsvd_version() -> *const c_char;
@@ -176,4 +219,12 @@ extern "C" {
         cap: i64, len: *mut i64) -> Status;
     pub fn lsvd_schedule_from_rotors(rotors: *const LsvdRotor, count: i64, channels: i64,
         target: i32, json: *mut c_char, cap: i64, len: *mut i64) -> Status;
+    pub fn lsvd_schedule_from_real_phaseflow(events: *const LsvdMziPhase, count: i64, channels: i64,
+        target: i32, json: *mut c_char, cap: i64, len: *mut i64) -> Status;
+    pub fn lsvd_schedule_binary_from_rotors(ctx: Ctx, rotors: *const LsvdRotor, count: i64, channels: i64,
+        target: i32, out: *mut c_void, cap: i64, len: *mut i64, flags: u32) -> Status;
+    pub fn lsvd_schedule_binary_from_real_phaseflow(events: *const LsvdMziPhase, count: i64, channels: i64,
+        target: i32, out: *mut c_void, cap: i64, len: *mut i64) -> Status;
+    pub fn lsvd_schedule_binary_to_json(frame: *const c_void, bytes: i64, json: *mut c_char, cap: i64,
+        len: *mut i64) -> Status;
 }

@@ -113,13 +113,14 @@ def test_rust_binding_matches_header():
 
     for name, args in c_fns.items():
         assert arity(r_fns[name]) == arity(args), name
-    c_structs = {m.group(2): re.findall(r"(\w+)\s*(?:,|;)", m.group(1))
+    c_structs = {m.group(2): re.findall(r"(\w+)\s*(?:\[\w+\])?\s*(?:,|;)", m.group(1))
                  for m in re.finditer(r"typedef struct\s*\w*\s*\{(.*?)\}\s*(\w+);", hdr, flags=re.S)}
     r_structs = {m.group(1): re.findall(r"pub (\w+):", m.group(2))
                  for m in re.finditer(r"pub struct (\w+)\s*\{(.*?)\}", rs, flags=re.S)}
     pairs = {"lsvd_diag": "LsvdDiag", "lsvd_rotor": "LsvdRotor", "lsvd_large_info": "LsvdLargeInfo",
              "lsvd_joint_params": "LsvdJointParams", "lsvd_joint_trace": "LsvdJointTrace",
-             "lsvd_triage": "LsvdTriage", "lsvd_polar_info": "LsvdPolarInfo"}
+             "lsvd_triage": "LsvdTriage", "lsvd_polar_info": "LsvdPolarInfo", "lsvd_mzi_phase": "LsvdMziPhase",
+             "lsvd_schedule_header": "LsvdScheduleHeader", "lsvd_schedule_record": "LsvdScheduleRecord"}
     assert set(pairs) == set(c_structs)
     for c_name, r_name in pairs.items():
         assert r_structs[r_name] == c_structs[c_name], c_name
