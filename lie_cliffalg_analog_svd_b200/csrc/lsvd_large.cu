@@ -377,33 +377,46 @@ __global__ void offnorm_final_kernel(const double* __restrict__ part, int nparts
     }
 }
 
-// Round-robin slot k (0..31) of round `round` over 64 indices: the circle
-// method of src/lie_svd_joint.rs:524-539 (index 63 fixed in slot 0).
-__device__ __forceinline__ void rr_slot(int round, int k, int& p, int& q) {
-    if (k == 0) {
-        p = PW - 1;
+// Slot k (0..31) of round `round` of a block-pair solve over the 64 local
+// indices (block lo = 0..31, block hi = 32..63).  Cross rounds (round 0..31)
+// pair lo index k with hi index 32 + (k + round) mod 32; the 31 inner rounds
+// pair the indices inside each block by the circle method of
+// src/lie_svd_joint.rs:524-539 over 32 (index 31 fixed; slots 0..15 in lo,
+// 16..31 the same pairs in hi).
+__device__ __forceinline__ void bp2_slot(bool inner, int round, int k, int& p, int& q) {
+    if (!inner) {
+        p = k;
+        q = BW + ((k + round) & (BW - 1));
+        return;
+    }
+    const int off = k < BW / 2 ? 0 : BW, kk = k & (BW / 2 - 1);
+    if (kk == 0) {
+        p = BW - 1;
         q = round;
     } else {
-        p = round + k;
-        p -= p >= PW - 1 ? PW - 1 : 0;
-        q = round - k;
-        q += q < 0 ? PW - 1 : 0;
+        p = round + kk;
+        p -= p >= BW - 1 ? BW - 1 : 0;
+        q = round - kk;
+        q += q < 0 ? BW - 1 : 0;
     }
+    p += off;
+    q += off;
 }
 
-// Two-sided route (1024 threads: the 63 rounds of a block sweep are the
+// Two-sided route (1024 threads: the rounds of a block-pair solve are the
 // critical path of every layer): gathers the 64 x 64 diagonal block M of
-// block pair blockIdx.x from P, diagonalises it (rotations of |a_pq| > tau,
-// the reference rotating every |a_pq| >= 1e-300, src/lie_svd_small.rs:
-// 233-235) and writes R / skip like solve_kernel.  Per round, warp 0
+// block pair blockIdx.x from P, rotates (|a_pq| > tau; the reference rotates
+// every |a_pq| >= 1e-300, src/lie_svd_small.rs:233-235, with the Rutishauser
+// tangent, :235-242) and writes R / skip like solve_kernel.  Every index pair
+// is visited once per sweep, as in the reference: its 32 cross rounds
+// (lo x hi pairs) on every layer, the 31 inner rounds of both blocks on
+// layer 0 only (every block is in a layer-0 pair).  Per round, warp 0
 // computes the 32 rotations (lane k <-> slot k); threads t < 528 update one
 // 2 x 2 block (slot a <= slot b) of the symmetric M as J_a^T M_ab J_b and
-// store it and its transpose; R never touches shared memory: thread
-// (warp w, lane k) keeps R's rows w and w + 32 at the two columns of slot k
-// in registers, rotates them, and hands them to the slots they occupy in the
-// next round by one shuffle each way (slot k's first index moves to slot
-// k - 1, its second to slot k + 1; the ends turn around).  After the 63
-// rounds of a sweep every column is back in its round-0 slot.
+// store it and its transpose.  R stays in registers: thread (warp w, lane k)
+// holds rows w and w + 32 of lo column k and of one hi column; a cross round
+// rotates the pair in place and passes the hi column to lane k - 1, an inner
+// round fetches the partner column of the same block from its lane.
 __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__ P, int64_t ldp, int nb, int layer,
                                                      double* __restrict__ Rg, int* __restrict__ skip,
                                                      SweepState* __restrict__ stt, double tau, int inner_max) {
@@ -414,6 +427,7 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
     __shared__ double red[32];
     __shared__ int s_flag;
     const int pair = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool with_inner = layer == 0;
     int Pb, Qb;
     block_pair(nb, layer, pair, Pb, Qb);
     for (int e = tid; e < PW * PW; e += 1024) {
@@ -421,17 +435,18 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
         Ms[i * MLD + j] = P[int64_t(pair_index(i, Pb, Qb)) * ldp + pair_index(j, Pb, Qb)];
     }
     __syncthreads();
+    // largest entry this solve may rotate: every off-diagonal on layer 0,
+    // the cross block otherwise
     double off = 0.0;
     for (int e = tid; e < PW * PW; e += 1024) {
         const int i = e >> 6, j = e & 63;
-        if (i < j) off = fmax(off, fabs(Ms[i * MLD + j]));
+        if (with_inner ? i < j : (i < BW && j >= BW)) off = fmax(off, fabs(Ms[i * MLD + j]));
     }
     off = block_max<1024>(off, red);
     if (!(off > tau)) {
         if (tid == 0) skip[pair] = 1;
         return;
     }
-    // this thread's block (ka, kb), ka <= kb, of the 32 x 32 slot triangle
     int ka = 0, kb = 0;
     const bool upd = tid < 32 * 33 / 2;
     if (upd) {
@@ -442,24 +457,24 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
         }
         kb = ka + rem;
     }
-    // R rows warp and warp + 32 at the round-0 columns of slot `lane`
-    int c0p, c0q;
-    rr_slot(0, lane, c0p, c0q);
-    double rp0 = warp == c0p ? 1.0 : 0.0, rq0 = warp == c0q ? 1.0 : 0.0;
-    double rp1 = warp + 32 == c0p ? 1.0 : 0.0, rq1 = warp + 32 == c0q ? 1.0 : 0.0;
+    // R rows warp, warp + 32 of lo column `lane` (l*) and hi column 32 + lane (h*)
+    double l0 = warp == lane ? 1.0 : 0.0, h0 = warp == lane + BW ? 1.0 : 0.0;
+    double l1 = warp + 32 == lane ? 1.0 : 0.0, h1 = warp + 32 == lane + BW ? 1.0 : 0.0;
     int cnt = 0, sweep = 0;
     for (; sweep < inner_max; ++sweep) {
         if (tid == 0) s_flag = 0;
         __syncthreads();
-        for (int round = 0; round < PW - 1; ++round) {
+        const int nround = with_inner ? (BW - 1) + BW : BW;
+        for (int it = 0; it < nround; ++it) {
+            const bool inner = with_inner && it < BW - 1;
+            const int round = inner ? it : it - (with_inner ? BW - 1 : 0);
             if (warp == 0) {
                 int p, qq;
-                rr_slot(round, lane, p, qq);
+                bp2_slot(inner, round, lane, p, qq);
                 const double app = Ms[p * MLD + p], aqq = Ms[qq * MLD + qq], apq = Ms[p * MLD + qq];
                 double c = 1.0, s = 0.0;
                 const bool rot = apq != 0.0 && fabs(apq) > tau;
                 if (rot) {
-                    // Rutishauser's tangent (src/lie_svd_small.rs:235-242)
                     const double zeta = (aqq - app) / (2.0 * apq);
                     const double t = fabs(zeta) > 1e150
                                          ? 0.5 / zeta
@@ -480,8 +495,8 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
                 const double ca = cs[ka], sa = sn[ka], cb = cs[kb], sb = sn[kb];
                 if (sa != 0.0 || sb != 0.0) {
                     int ra, rb, ca_, cb_;
-                    rr_slot(round, ka, ra, rb);
-                    rr_slot(round, kb, ca_, cb_);
+                    bp2_slot(inner, round, ka, ra, rb);
+                    bp2_slot(inner, round, kb, ca_, cb_);
                     const double x = Ms[ra * MLD + ca_], y = Ms[ra * MLD + cb_];
                     const double z = Ms[rb * MLD + ca_], w = Ms[rb * MLD + cb_];
                     const double x1 = cb * x - sb * y, y1 = sb * x + cb * y;
@@ -501,20 +516,40 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
                     }
                 }
             }
-            {
-                // R <- R J on the registers, then the move to the next round's slots
-                const double c = cs[lane], s = sn[lane];
-                const double u0 = c * rp0 - s * rq0, v0 = s * rp0 + c * rq0;
-                const double u1 = c * rp1 - s * rq1, v1 = s * rp1 + c * rq1;
-                const double dp0 = __shfl_down_sync(0xffffffffu, u0, 1), dp1 = __shfl_down_sync(0xffffffffu, u1, 1);
-                const double uq0 = __shfl_up_sync(0xffffffffu, v0, 1), uq1 = __shfl_up_sync(0xffffffffu, v1, 1);
-                if (lane == 0) {
-                    rp0 = u0, rp1 = u1, rq0 = dp0, rq1 = dp1;
-                } else if (lane == 31) {
-                    rp0 = v0, rp1 = v1, rq0 = uq0, rq1 = uq1;
+            if (inner) {
+                // lane's index x in its block: role and partner in the circle method
+                int k, partner;
+                bool role_p;
+                if (lane == BW - 1) {
+                    k = 0, role_p = true, partner = round;
+                } else if (lane == round) {
+                    k = 0, role_p = false, partner = BW - 1;
                 } else {
-                    rp0 = dp0, rp1 = dp1, rq0 = uq0, rq1 = uq1;
+                    int d = lane - round;
+                    d += d < 0 ? BW - 1 : 0;
+                    role_p = d <= BW / 2 - 1;
+                    k = role_p ? d : BW - 1 - d;
+                    partner = role_p ? round - k : round + k;
+                    partner += partner < 0 ? BW - 1 : 0;
+                    partner -= partner >= BW - 1 ? BW - 1 : 0;
                 }
+                const double cl = cs[k], sl = sn[k], ch = cs[BW / 2 + k], sh = sn[BW / 2 + k];
+                const double pl0 = __shfl_sync(0xffffffffu, l0, partner), pl1 = __shfl_sync(0xffffffffu, l1, partner);
+                const double ph0 = __shfl_sync(0xffffffffu, h0, partner), ph1 = __shfl_sync(0xffffffffu, h1, partner);
+                if (role_p) {
+                    l0 = cl * l0 - sl * pl0, l1 = cl * l1 - sl * pl1;
+                    h0 = ch * h0 - sh * ph0, h1 = ch * h1 - sh * ph1;
+                } else {
+                    l0 = sl * pl0 + cl * l0, l1 = sl * pl1 + cl * l1;
+                    h0 = sh * ph0 + ch * h0, h1 = sh * ph1 + ch * h1;
+                }
+            } else {
+                const double c = cs[lane], s = sn[lane];
+                const double u0 = c * l0 - s * h0, v0 = s * l0 + c * h0;
+                const double u1 = c * l1 - s * h1, v1 = s * l1 + c * h1;
+                l0 = u0, l1 = u1;
+                h0 = __shfl_sync(0xffffffffu, v0, (lane + 1) & 31);
+                h1 = __shfl_sync(0xffffffffu, v1, (lane + 1) & 31);
             }
             __syncthreads();
         }
@@ -524,10 +559,10 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
     }
     const int sw = sweep == inner_max ? inner_max + 1 : sweep + 1;
     double* R = Rg + int64_t(pair) * (PW * PW);
-    R[warp * PW + c0p] = rp0;
-    R[warp * PW + c0q] = rq0;
-    R[(warp + 32) * PW + c0p] = rp1;
-    R[(warp + 32) * PW + c0q] = rq1;
+    R[warp * PW + lane] = l0;
+    R[warp * PW + BW + lane] = h0;
+    R[(warp + 32) * PW + lane] = l1;
+    R[(warp + 32) * PW + BW + lane] = h1;
     if (tid == 0) {
         skip[pair] = 0;
         stt->rotated = 1;
