@@ -178,154 +178,25 @@ __device__ __forceinline__ double pair_scale(double mii, double mjj, double S) {
 
 // Largest scaled off-diagonal |M_ij| / pair_scale over i < j of the 64 x 64
 // Gram in shared memory.
-__device__ __forceinline__ double scaled_offdiag(const double* Ms, double S, double* red) {
-    double off = 0.0;
-    for (int e = threadIdx.x; e < PW * PW; e += 256) {  // 256-thread CTAs
+template <int NT>
+__device__ __forceinline__ void scaled_offdiag(const double* Ms, double S, double* red, double& all, double& cross) {
+    double off = 0.0, offc = 0.0;
+    for (int e = threadIdx.x; e < PW * PW; e += NT) {
         const int i = e >> 6, j = e & 63;
         if (i < j) {
             const double d = pair_scale(Ms[i * MLD + i], Ms[j * MLD + j], S);
-            if (d > 0.0) off = fmax(off, fabs(Ms[i * MLD + j]) / d);
+            if (d > 0.0) {
+                const double v = fabs(Ms[i * MLD + j]) / d;
+                off = fmax(off, v);
+                if (i < BW && j >= BW) offc = fmax(offc, v);
+            }
         }
     }
-    return block_max<256>(off, red);
+    all = block_max<NT>(off, red);
+    cross = block_max<NT>(offc, red);
 }
 
-// Cyclic two-sided Jacobi sweeps (at most inner_max, parallel round-robin
-// order over the 64 indices) on the symmetric 64 x 64 matrix Ms, accumulating
-// the rotations into Rs (which holds I on entry).  rotate(app, aqq, apq)
-// decides whether pair (p, q) is rotated; the sweeps stop after one in which
-// no pair was.  Returns the sweeps run (inner_max + 1 when the cap was hit)
-// and adds the rotations to *cnt.
-template <int NT, class Rot>
-__device__ int inner_jacobi(double* Ms, double* Rs, int inner_max, Rot rotate, double* cs, double* sn, int* pa,
-                            int* qa, int* flag, int* cnt) {
-    const int tid = threadIdx.x;
-    int sweep = 0;
-    for (; sweep < inner_max; ++sweep) {
-        if (tid == 0) *flag = 0;
-        __syncthreads();
-        for (int round = 0; round < PW - 1; ++round) {
-            if (tid < 32) {
-                int p, qq;
-                // circle method over 64 indices (src/lie_svd_joint.rs:524-539)
-                if (tid == 0) {
-                    p = PW - 1;
-                    qq = round;
-                } else {
-                    p = (round + tid) % (PW - 1);
-                    qq = (round + PW - 1 - tid) % (PW - 1);
-                }
-                const double app = Ms[p * MLD + p], aqq = Ms[qq * MLD + qq], apq = Ms[p * MLD + qq];
-                double c = 1.0, s = 0.0;
-                const bool rot = apq != 0.0 && rotate(app, aqq, apq);
-                if (rot) {
-                    // Rutishauser's tangent (src/lie_svd_small.rs:235-242)
-                    const double zeta = (aqq - app) / (2.0 * apq);
-                    const double t = fabs(zeta) > 1e150
-                                         ? 0.5 / zeta
-                                         : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    c = rsqrt(1.0 + t * t);
-                    s = t * c;
-                }
-                // one count per round instead of a contended shared atomic per rotation
-                const unsigned msk = __ballot_sync(0xffffffffu, rot);
-                if (tid == 0 && msk) {
-                    *cnt += __popc(msk);
-                    *flag = 1;
-                }
-                cs[tid] = c;
-                sn[tid] = s;
-                pa[tid] = p;
-                qa[tid] = qq;
-            }
-            __syncthreads();
-            // M <- J^T M J over 32 x 32 independent 2 x 2 blocks
-            for (int b = tid; b < 32 * 32; b += NT) {
-                const int ka = b >> 5, kb = b & 31;
-                const double ca = cs[ka], sa = sn[ka], cb = cs[kb], sb = sn[kb];
-                if (sa == 0.0 && sb == 0.0) continue;
-                const int ra = pa[ka], rb = qa[ka], ca_ = pa[kb], cb_ = qa[kb];
-                const double x = Ms[ra * MLD + ca_], y = Ms[ra * MLD + cb_];
-                const double z = Ms[rb * MLD + ca_], w = Ms[rb * MLD + cb_];
-                const double x1 = cb * x - sb * y, y1 = sb * x + cb * y;
-                const double z1 = cb * z - sb * w, w1 = sb * z + cb * w;
-                double x2 = ca * x1 - sa * z1, y2 = ca * y1 - sa * w1;
-                double z2 = sa * x1 + ca * z1, w2 = sa * y1 + ca * w1;
-                if (ka == kb) y2 = z2 = 0.0;  // the pair this rotation annihilates
-                Ms[ra * MLD + ca_] = x2;
-                Ms[ra * MLD + cb_] = y2;
-                Ms[rb * MLD + ca_] = z2;
-                Ms[rb * MLD + cb_] = w2;
-            }
-            // R <- R J
-            for (int t = tid; t < PW * 32; t += NT) {
-                const int r = t >> 5, k = t & 31;
-                const double c = cs[k], s = sn[k];
-                if (s == 0.0) continue;
-                const double u = Rs[r * MLD + pa[k]], v = Rs[r * MLD + qa[k]];
-                Rs[r * MLD + pa[k]] = c * u - s * v;
-                Rs[r * MLD + qa[k]] = s * u + c * v;
-            }
-            __syncthreads();
-        }
-        const int any = *flag;
-        __syncthreads();
-        if (!any) break;
-    }
-    return sweep == inner_max ? inner_max + 1 : sweep + 1;
-}
 
-// One-sided route: sums the Gram partials of a block pair, tests it, and
-// diagonalises the Gram into the rotation R (64 x 64, row-major, Rg[pair]).
-// skip[pair] = 1 when the pair needs no rotation.
-__global__ void __launch_bounds__(256) solve_kernel(const double* __restrict__ Mpart, int nchunk,
-                                                    double* __restrict__ Rg, int* __restrict__ skip,
-                                                    SweepState* __restrict__ stt, double tol, int inner_max) {
-    if (stt->converged) return;
-    extern __shared__ __align__(16) double ssmem[];
-    double* Ms = ssmem;             // 64 x 64 Gram, leading dimension 65
-    double* Rs = ssmem + PW * MLD;  // 64 x 64 rotation
-    __shared__ double cs[32], sn[32];
-    __shared__ int pa[32], qa[32];
-    __shared__ double red[8];
-    __shared__ int s_cnt, s_flag;
-    const int pair = blockIdx.x, tid = threadIdx.x;
-    const double* mp = Mpart + int64_t(pair) * nchunk * (PW * PW);
-    for (int e = tid; e < PW * PW; e += 256) {
-        double v = 0.0;
-        for (int c = 0; c < nchunk; ++c) v += mp[int64_t(c) * (PW * PW) + e];
-        Ms[(e >> 6) * MLD + (e & 63)] = v;
-        Rs[(e >> 6) * MLD + (e & 63)] = (e >> 6) == (e & 63) ? 1.0 : 0.0;
-    }
-    if (tid == 0) s_cnt = 0;
-    __syncthreads();
-    const double S = stt->scale2;
-    {
-        double dmax = 0.0;
-        for (int i = tid; i < PW; i += 256) dmax = fmax(dmax, Ms[i * MLD + i]);
-        dmax = block_max<256>(dmax, red);
-        if (tid == 0)
-            atomicMax(&stt->next_scale2, static_cast<unsigned long long>(__double_as_longlong(dmax)));
-    }
-    const double off0 = scaled_offdiag(Ms, S, red);
-    if (tid == 0) atomicMax(&stt->max_off, static_cast<unsigned long long>(__double_as_longlong(off0)));
-    if (!(off0 > tol)) {  // also catches NaN: nothing to rotate
-        if (tid == 0) skip[pair] = 1;
-        return;
-    }
-    const int sw = inner_jacobi<256>(
-        Ms, Rs, inner_max,
-        [&](double app, double aqq, double apq) { return fabs(apq) > tol * pair_scale(app, aqq, S); }, cs, sn,
-        pa, qa, &s_flag, &s_cnt);
-    double* R = Rg + int64_t(pair) * (PW * PW);
-    for (int e = tid; e < PW * PW; e += 256) R[e] = Rs[(e >> 6) * MLD + (e & 63)];
-    if (tid == 0) {
-        skip[pair] = 0;
-        stt->rotated = 1;
-        atomicAdd(&stt->rotations, (unsigned long long)s_cnt);
-        if (sw > inner_max) atomicAdd(&stt->inner_cap, 1);
-    }
-}
 
 // Index of column/row `c` (0..63) of block pair (P, Q) in the full matrix.
 __device__ __forceinline__ int pair_index(int c, int P, int Q) { return hrow_of(c, P, Q); }
@@ -403,50 +274,18 @@ __device__ __forceinline__ void bp2_slot(bool inner, int round, int k, int& p, i
     q += off;
 }
 
-// Two-sided route (1024 threads: the rounds of a block-pair solve are the
-// critical path of every layer): gathers the 64 x 64 diagonal block M of
-// block pair blockIdx.x from P, rotates (|a_pq| > tau; the reference rotates
-// every |a_pq| >= 1e-300, src/lie_svd_small.rs:233-235, with the Rutishauser
-// tangent, :235-242) and writes R / skip like solve_kernel.  Every index pair
-// is visited once per sweep, as in the reference: its 32 cross rounds
-// (lo x hi pairs) on every layer, the 31 inner rounds of both blocks on
-// layer 0 only (every block is in a layer-0 pair).  Per round, warp 0
-// computes the 32 rotations (lane k <-> slot k); threads t < 528 update one
-// 2 x 2 block (slot a <= slot b) of the symmetric M as J_a^T M_ab J_b and
-// store it and its transpose.  R stays in registers: thread (warp w, lane k)
-// holds rows w and w + 32 of lo column k and of one hi column; a cross round
-// rotates the pair in place and passes the hi column to lane k - 1, an inner
-// round fetches the partner column of the same block from its lane.
-__global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__ P, int64_t ldp, int nb, int layer,
-                                                     double* __restrict__ Rg, int* __restrict__ skip,
-                                                     SweepState* __restrict__ stt, double tau, int inner_max) {
-    if (stt->converged) return;
-    extern __shared__ __align__(16) double ssmem[];
-    double* Ms = ssmem;
-    __shared__ double cs[32], sn[32];
-    __shared__ double red[32];
-    __shared__ int s_flag;
-    const int pair = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool with_inner = layer == 0;
-    int Pb, Qb;
-    block_pair(nb, layer, pair, Pb, Qb);
-    for (int e = tid; e < PW * PW; e += 1024) {
-        const int i = e >> 6, j = e & 63;
-        Ms[i * MLD + j] = P[int64_t(pair_index(i, Pb, Qb)) * ldp + pair_index(j, Pb, Qb)];
-    }
-    __syncthreads();
-    // largest entry this solve may rotate: every off-diagonal on layer 0,
-    // the cross block otherwise
-    double off = 0.0;
-    for (int e = tid; e < PW * PW; e += 1024) {
-        const int i = e >> 6, j = e & 63;
-        if (with_inner ? i < j : (i < BW && j >= BW)) off = fmax(off, fabs(Ms[i * MLD + j]));
-    }
-    off = block_max<1024>(off, red);
-    if (!(off > tau)) {
-        if (tid == 0) skip[pair] = 1;
-        return;
-    }
+// The rounds of one block-pair solve by a 1024-thread CTA (see
+// solve2_kernel): cross rounds on every layer, the inner rounds of both
+// blocks first when with_inner; up to inner_max passes while some pair
+// rotates.  rotate(app, aqq, apq) decides a pair.  On return this thread
+// holds rows warp, warp + 32 of R's lo column `lane` (l0, l1) and hi column
+// 32 + lane (h0, h1); *cnt (lane 0 of warp 0) counts the rotations.
+// Returns the passes run (inner_max + 1 when the cap was hit).
+template <class Rot>
+__device__ int pair_rounds(double* Ms, bool with_inner, int inner_max, Rot rotate, double* cs, double* sn,
+                           int* s_flag_p, int& cnt, double& l0, double& l1, double& h0, double& h1) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int& s_flag = *s_flag_p;
     int ka = 0, kb = 0;
     const bool upd = tid < 32 * 33 / 2;
     if (upd) {
@@ -457,10 +296,9 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
         }
         kb = ka + rem;
     }
-    // R rows warp, warp + 32 of lo column `lane` (l*) and hi column 32 + lane (h*)
-    double l0 = warp == lane ? 1.0 : 0.0, h0 = warp == lane + BW ? 1.0 : 0.0;
-    double l1 = warp + 32 == lane ? 1.0 : 0.0, h1 = warp + 32 == lane + BW ? 1.0 : 0.0;
-    int cnt = 0, sweep = 0;
+    l0 = warp == lane ? 1.0 : 0.0, h0 = warp == lane + BW ? 1.0 : 0.0;
+    l1 = warp + 32 == lane ? 1.0 : 0.0, h1 = warp + 32 == lane + BW ? 1.0 : 0.0;
+    int sweep = 0;
     for (; sweep < inner_max; ++sweep) {
         if (tid == 0) s_flag = 0;
         __syncthreads();
@@ -473,7 +311,7 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
                 bp2_slot(inner, round, lane, p, qq);
                 const double app = Ms[p * MLD + p], aqq = Ms[qq * MLD + qq], apq = Ms[p * MLD + qq];
                 double c = 1.0, s = 0.0;
-                const bool rot = apq != 0.0 && fabs(apq) > tau;
+                const bool rot = apq != 0.0 && rotate(app, aqq, apq);
                 if (rot) {
                     const double zeta = (aqq - app) / (2.0 * apq);
                     const double t = fabs(zeta) > 1e150
@@ -557,7 +395,116 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
         __syncthreads();
         if (!any) break;
     }
-    const int sw = sweep == inner_max ? inner_max + 1 : sweep + 1;
+    return sweep == inner_max ? inner_max + 1 : sweep + 1;
+}
+
+// Two-sided route (1024 threads: the rounds of a block-pair solve are the
+// critical path of every layer): gathers the 64 x 64 diagonal block M of
+// block pair blockIdx.x from P, rotates (|a_pq| > tau; the reference rotates
+// every |a_pq| >= 1e-300, src/lie_svd_small.rs:233-235, with the Rutishauser
+// tangent, :235-242) and writes R / skip like solve_kernel.  Every index pair
+// is visited once per sweep, as in the reference: its 32 cross rounds
+// (lo x hi pairs) on every layer, the 31 inner rounds of both blocks on
+// layer 0 only (every block is in a layer-0 pair).  Per round, warp 0
+// computes the 32 rotations (lane k <-> slot k); threads t < 528 update one
+// 2 x 2 block (slot a <= slot b) of the symmetric M as J_a^T M_ab J_b and
+// store it and its transpose.  R stays in registers: thread (warp w, lane k)
+// holds rows w and w + 32 of lo column k and of one hi column; a cross round
+// rotates the pair in place and passes the hi column to lane k - 1, an inner
+// round fetches the partner column of the same block from its lane.
+__global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__ P, int64_t ldp, int nb, int layer,
+                                                     double* __restrict__ Rg, int* __restrict__ skip,
+                                                     SweepState* __restrict__ stt, double tau, int inner_max) {
+    if (stt->converged) return;
+    extern __shared__ __align__(16) double ssmem[];
+    double* Ms = ssmem;
+    __shared__ double cs[32], sn[32];
+    __shared__ double red[32];
+    __shared__ int s_flag;
+    const int pair = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool with_inner = layer == 0;
+    int Pb, Qb;
+    block_pair(nb, layer, pair, Pb, Qb);
+    for (int e = tid; e < PW * PW; e += 1024) {
+        const int i = e >> 6, j = e & 63;
+        Ms[i * MLD + j] = P[int64_t(pair_index(i, Pb, Qb)) * ldp + pair_index(j, Pb, Qb)];
+    }
+    __syncthreads();
+    // largest entry this solve may rotate: every off-diagonal on layer 0,
+    // the cross block otherwise
+    double off = 0.0;
+    for (int e = tid; e < PW * PW; e += 1024) {
+        const int i = e >> 6, j = e & 63;
+        if (with_inner ? i < j : (i < BW && j >= BW)) off = fmax(off, fabs(Ms[i * MLD + j]));
+    }
+    off = block_max<1024>(off, red);
+    if (!(off > tau)) {
+        if (tid == 0) skip[pair] = 1;
+        return;
+    }
+    double l0, l1, h0, h1;
+    int cnt = 0;
+    const int sw = pair_rounds(
+        Ms, with_inner, inner_max, [&](double, double, double apq) { return fabs(apq) > tau; }, cs, sn, &s_flag, cnt,
+        l0, l1, h0, h1);
+    double* R = Rg + int64_t(pair) * (PW * PW);
+    R[warp * PW + lane] = l0;
+    R[warp * PW + BW + lane] = h0;
+    R[(warp + 32) * PW + lane] = l1;
+    R[(warp + 32) * PW + BW + lane] = h1;
+    if (tid == 0) {
+        skip[pair] = 0;
+        stt->rotated = 1;
+        atomicAdd(&stt->rotations, (unsigned long long)cnt);
+        if (sw > inner_max) atomicAdd(&stt->inner_cap, 1);
+    }
+}
+
+// One-sided route: sums the Gram partials of a block pair, tests it, and
+// rotates its pairs as solve2_kernel does (pair_rounds; a pair rotates when
+// |g_pq| > tol * pair_scale), writing R (64 x 64, row-major, Rg[pair]) and
+// skip[pair] = 1 when no pair this solve visits needs a rotation.  The
+// sweep's convergence measure is the largest scaled off-diagonal over every
+// pair of every Gram the sweep forms.
+__global__ void __launch_bounds__(1024) solve_kernel(const double* __restrict__ Mpart, int nchunk, int layer,
+                                                     double* __restrict__ Rg, int* __restrict__ skip,
+                                                     SweepState* __restrict__ stt, double tol, int inner_max) {
+    if (stt->converged) return;
+    extern __shared__ __align__(16) double ssmem[];
+    double* Ms = ssmem;  // 64 x 64 Gram, leading dimension 65
+    __shared__ double cs[32], sn[32];
+    __shared__ double red[32];
+    __shared__ int s_flag;
+    const int pair = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool with_inner = layer == 0;
+    const double* mp = Mpart + int64_t(pair) * nchunk * (PW * PW);
+    for (int e = tid; e < PW * PW; e += 1024) {
+        double v = 0.0;
+        for (int c = 0; c < nchunk; ++c) v += mp[int64_t(c) * (PW * PW) + e];
+        Ms[(e >> 6) * MLD + (e & 63)] = v;
+    }
+    __syncthreads();
+    const double S = stt->scale2;
+    {
+        double dmax = 0.0;
+        for (int i = tid; i < PW; i += 1024) dmax = fmax(dmax, Ms[i * MLD + i]);
+        dmax = block_max<1024>(dmax, red);
+        if (tid == 0)
+            atomicMax(&stt->next_scale2, static_cast<unsigned long long>(__double_as_longlong(dmax)));
+    }
+    double off_all, off_cross;
+    scaled_offdiag<1024>(Ms, S, red, off_all, off_cross);
+    if (tid == 0) atomicMax(&stt->max_off, static_cast<unsigned long long>(__double_as_longlong(off_all)));
+    if (!((with_inner ? off_all : off_cross) > tol)) {  // also catches NaN: nothing to rotate
+        if (tid == 0) skip[pair] = 1;
+        return;
+    }
+    double l0, l1, h0, h1;
+    int cnt = 0;
+    const int sw = pair_rounds(
+        Ms, with_inner, inner_max,
+        [&](double app, double aqq, double apq) { return fabs(apq) > tol * pair_scale(app, aqq, S); }, cs, sn,
+        &s_flag, cnt, l0, l1, h0, h1);
     double* R = Rg + int64_t(pair) * (PW * PW);
     R[warp * PW + lane] = l0;
     R[warp * PW + BW + lane] = h0;
@@ -976,8 +923,7 @@ __global__ void transpose_kernel(int rows, int cols, const double* in, int64_t l
 
 constexpr int kApplySmem = 3 * PW * XLD * 8;  // R + two stages: 104448 bytes
 constexpr int kGramSmem = 3 * PW * GLD * 8;   // three stages: 55296 bytes
-constexpr int kSolveSmem = 2 * PW * MLD * 8;  // M and R: 66560 bytes (solve_kernel)
-constexpr int kSolve2Smem = PW * MLD * 8;    // M: 33280 bytes
+constexpr int kSolve2Smem = PW * MLD * 8;  // M: 33280 bytes (solve_kernel, solve2_kernel)
 constexpr int kTwoSmem = 3 * PW * XLD * 8;    // P_ab / T, R_a, R_b: 104448 bytes
 
 struct EventTimer {
@@ -1034,7 +980,7 @@ static lsvd_status run_sweeps(lsvd_context* ctx, double* H, int64_t ldh, int gm,
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // hinit is reused for the sweep reads below
     if (e == cudaSuccess) e = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGramSmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolve2Smem);
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: sweep setup");
     // one sweep = nb - 1 layers of (gram, solve, apply) + the sweep-end test, captured once
     cudaGraph_t graph = nullptr;
@@ -1043,7 +989,7 @@ static lsvd_status run_sweeps(lsvd_context* ctx, double* H, int64_t ldh, int gm,
         return lsvd_ctx_cuda(ctx, e, "large: begin capture");
     for (int layer = 0; layer < nb - 1; ++layer) {
         gram_kernel<<<dim3(npairs, nchunk), 256, kGramSmem, st>>>(H, ldh, nb, layer, kchunk, gpad, Mpart, stt);
-        solve_kernel<<<npairs, 256, kSolveSmem, st>>>(Mpart, nchunk, Rg, skip, stt, tol, inner_max);
+        solve_kernel<<<npairs, 1024, kSolve2Smem, st>>>(Mpart, nchunk, layer, Rg, skip, stt, tol, inner_max);
         apply_kernel<<<dim3(npairs, napply), 256, kApplySmem, st>>>(H, ldh, nb, layer, rows, Rg, skip, stt);
     }
     sweep_end_kernel<<<1, 1, 0, st>>>(stt, tol_conv);
