@@ -50,6 +50,12 @@ struct Mat {
     void store(double* p) const { std::memcpy(p, a.data(), sizeof(double) * a.size()); }
 };
 
+// ndarray's `dot` (ndarray 0.15.6 over matrixmultiply 0.3.11, the versions
+// of the reference's Cargo.lock) on an x86-64 host with FMA: the dgemm
+// micro-kernel accumulates every C(i, j) over k = 0, 1, ... in order with a
+// fused multiply-add from zero, then scales by alpha = 1 (exact).  The products
+// below keep that order and rounding, so rounding-level outputs (orthogonality,
+// reconstruction residuals) reproduce the reference's printed ones.
 // C = A * B
 Mat matmul(const Mat& A, const Mat& B) {
     Mat C(A.r, B.c);
@@ -58,7 +64,7 @@ Mat matmul(const Mat& A, const Mat& B) {
             const double aik = A(i, k);
             const double* brow = &B.a[size_t(k * B.c)];
             double* crow = &C.a[size_t(i * C.c)];
-            for (int64_t j = 0; j < B.c; ++j) crow[j] += aik * brow[j];
+            for (int64_t j = 0; j < B.c; ++j) crow[j] = std::fma(aik, brow[j], crow[j]);
         }
     return C;
 }
@@ -70,7 +76,7 @@ Mat matmul_tn(const Mat& A, const Mat& B) {
             const double aki = A(k, i);
             const double* brow = &B.a[size_t(k * B.c)];
             double* crow = &C.a[size_t(i * C.c)];
-            for (int64_t j = 0; j < B.c; ++j) crow[j] += aki * brow[j];
+            for (int64_t j = 0; j < B.c; ++j) crow[j] = std::fma(aki, brow[j], crow[j]);
         }
     return C;
 }
@@ -904,6 +910,15 @@ int64_t oracle_schedule_from_orthogonal(int64_t d, const double* V, int64_t cap,
 }
 
 // Rust `{:.17e}`: 17 fractional digits, exponent without '+' or zero padding.
+// ndarray `a.dot(&b)` of row-major m x k and k x n operands (the product
+// order of matmul above); used to rebuild inputs the reference constructs
+// with dot products.
+int oracle_dot(int64_t m, int64_t k, int64_t n, const double* A, const double* B, double* C) {
+    if (m < 0 || k < 0 || n < 0 || (m * k > 0 && !A) || (k * n > 0 && !B) || (m * n > 0 && !C)) return -1;
+    matmul(Mat::from(m, k, A), Mat::from(k, n, B)).store(C);
+    return 0;
+}
+
 int oracle_fmt_e17(double x, char* buf, int64_t cap) {
     char tmp[64];
     std::string s;

@@ -120,6 +120,10 @@ int64_t oracle_schedule_from_orthogonal(int64_t d, const double* V, int64_t cap,
 
 /* Formats a Rust `{:.17e}` float (src/lie_svd_compiler.rs:227) into buf.
  * Returns the string length. */
+/* ndarray `a.dot(&b)` (row-major m x k times k x n) in the reference's product
+ * order: sequential fused multiply-adds over k. */
+int oracle_dot(int64_t m, int64_t k, int64_t n, const double* A, const double* B, double* C);
+
 int oracle_fmt_e17(double x, char* buf, int64_t cap);
 
 #ifdef __cplusplus

@@ -68,6 +68,7 @@ def lib():
         _lib.oracle_triage.argtypes = [C.c_int64, C.c_int64, V, V, V]
         _lib.oracle_svd_batch.restype = C.c_int64
         _lib.oracle_svd_batch.argtypes = [C.c_int64, V, V, V, V, V, V, V, V, C.c_int32]
+        _lib.oracle_dot.argtypes = [C.c_int64, C.c_int64, C.c_int64, P, P, P]
     return _lib
 
 
@@ -285,6 +286,39 @@ class metrics:  # noqa: N801 -- mirrors the Rust module name
         return SvdMetrics(out[0], out[1], out[2],
                           None if sigma_ref is None else out[3],
                           None if sigma_ref is None else out[4])
+
+
+def dot(a, b) -> np.ndarray:
+    """ndarray ``a.dot(&b)`` in the reference's product order (sequential
+    fused multiply-adds over k, matrixmultiply 0.3.11's f64 kernel)."""
+    a, b = _c(a), _c(b)
+    m, k = a.shape
+    k2, n = b.shape
+    assert k == k2
+    c = np.empty((m, n))
+    assert lib().oracle_dot(C.c_int64(m), C.c_int64(k), C.c_int64(n), _p(a), _p(b), _p(c)) == 0
+    return c
+
+
+def _next_centered(state: list) -> float:
+    """``next_centered`` of the reference's stress binary
+    (src/bin/stress_cpu.rs:829-833): a 64-bit LCG, top 53 bits, minus 1/2."""
+    state[0] = (state[0] * 6364136223846793005 + 1) & 0xFFFFFFFFFFFFFFFF
+    return (state[0] >> 11) / float(1 << 53) - 0.5
+
+
+def deterministic_orthogonal(n: int, state: list) -> np.ndarray:
+    """``deterministic_orthogonal`` (src/bin/stress_cpu.rs:805-827): LCG
+    entries in row-major order, then Gram-Schmidt over the columns with the
+    reference's sequential sums (each product rounded, summed left to right)."""
+    q = np.array([_next_centered(state) for _ in range(n * n)]).reshape(n, n)
+    for j in range(n):
+        for k in range(j):
+            d = np.cumsum(q[:, j] * q[:, k])[-1]
+            q[:, j] -= d * q[:, k]
+        nrm = max(float(np.sqrt(np.cumsum(q[:, j] * q[:, j])[-1])), 1e-300)
+        q[:, j] /= nrm
+    return q
 
 
 def fmt_e17(x: float) -> str:
