@@ -5,11 +5,12 @@
 // against and the timed CPU baseline; the product never links or calls it.
 //
 // Each function names the Rust lines it follows.  The arithmetic is the
-// reference's: same iteration formulas, thresholds, loop orders and caps.
-// The one systematic difference is GEMM summation order: the reference's
-// `.dot` goes through ndarray 0.15.6 -> matrixmultiply 0.3.11 (a blocked
-// kernel), this file uses plain i-k-j loops, so results agree to rounding
-// (~1e-15 relative), not bitwise.
+// reference's: same iteration formulas, thresholds, loop orders and caps, and
+// the reference's `.dot` (ndarray 0.15.6 -> matrixmultiply 0.3.11) restated
+// in its per-element order, sequential fused multiply-adds over k.  Pinned:
+// the reference's printed rounding statistics and rotation counts for its
+// RNG-free inputs are reproduced to every printed digit
+// (tests/test_oracle_pinned.py).
 #include "lsvd_oracle.h"
 
 #include <algorithm>
