@@ -52,33 +52,48 @@ struct Mat {
 };
 
 // ndarray's `dot` (ndarray 0.15.6 over matrixmultiply 0.3.11, the versions
-// of the reference's Cargo.lock) on an x86-64 host with FMA: the dgemm
-// micro-kernel accumulates every C(i, j) over k = 0, 1, ... in order with a
-// fused multiply-add from zero, then scales by alpha = 1 (exact).  The products
-// below keep that order and rounding, so rounding-level outputs (orthogonality,
-// reconstruction residuals) reproduce the reference's printed ones.
+// of the reference's Cargo.lock): the dgemm micro-kernel accumulates every
+// C(i, j) over k = 0, 1, ... in order from zero, then scales by alpha = 1
+// (exact) -- with a fused multiply-add per k on hosts with FMA (the default
+// here), with a multiply then an add on hosts without (oracle_set_dot_fma(0)).
+// The products below keep that order and rounding, so rounding-level outputs
+// (orthogonality, reconstruction residuals) reproduce the reference's printed
+// ones on either kind of host.
+bool g_dot_fma = true;
+
+template <bool FMA>
+void mm_rows(const Mat& A, const Mat& B, Mat& C, bool trans_a) {
+    const int64_t kk = trans_a ? A.r : A.c, mi = trans_a ? A.c : A.r;
+    for (int64_t i = 0; i < mi; ++i)
+        for (int64_t k = 0; k < kk; ++k) {
+            const double a = trans_a ? A(k, i) : A(i, k);
+            const double* brow = &B.a[size_t(k * B.c)];
+            double* crow = &C.a[size_t(i * C.c)];
+            for (int64_t j = 0; j < B.c; ++j) {
+                if (FMA)
+                    crow[j] = std::fma(a, brow[j], crow[j]);
+                else
+                    crow[j] += a * brow[j];
+            }
+        }
+}
+
 // C = A * B
 Mat matmul(const Mat& A, const Mat& B) {
     Mat C(A.r, B.c);
-    for (int64_t i = 0; i < A.r; ++i)
-        for (int64_t k = 0; k < A.c; ++k) {
-            const double aik = A(i, k);
-            const double* brow = &B.a[size_t(k * B.c)];
-            double* crow = &C.a[size_t(i * C.c)];
-            for (int64_t j = 0; j < B.c; ++j) crow[j] = std::fma(aik, brow[j], crow[j]);
-        }
+    if (g_dot_fma)
+        mm_rows<true>(A, B, C, false);
+    else
+        mm_rows<false>(A, B, C, false);
     return C;
 }
 // C = A^T * B
 Mat matmul_tn(const Mat& A, const Mat& B) {
     Mat C(A.c, B.c);
-    for (int64_t k = 0; k < A.r; ++k)
-        for (int64_t i = 0; i < A.c; ++i) {
-            const double aki = A(k, i);
-            const double* brow = &B.a[size_t(k * B.c)];
-            double* crow = &C.a[size_t(i * C.c)];
-            for (int64_t j = 0; j < B.c; ++j) crow[j] = std::fma(aki, brow[j], crow[j]);
-        }
+    if (g_dot_fma)
+        mm_rows<true>(A, B, C, true);
+    else
+        mm_rows<false>(A, B, C, true);
     return C;
 }
 
@@ -911,6 +926,8 @@ int64_t oracle_schedule_from_orthogonal(int64_t d, const double* V, int64_t cap,
 }
 
 // Rust `{:.17e}`: 17 fractional digits, exponent without '+' or zero padding.
+void oracle_set_dot_fma(int32_t on) { g_dot_fma = on != 0; }
+
 // ndarray `a.dot(&b)` of row-major m x k and k x n operands (the product
 // order of matmul above); used to rebuild inputs the reference constructs
 // with dot products.

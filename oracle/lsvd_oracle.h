@@ -120,6 +120,11 @@ int64_t oracle_schedule_from_orthogonal(int64_t d, const double* V, int64_t cap,
 
 /* Formats a Rust `{:.17e}` float (src/lie_svd_compiler.rs:227) into buf.
  * Returns the string length. */
+/* Product rounding of every ndarray `dot` the oracle restates: 1 (default) =
+ * fused multiply-add per k (matrixmultiply's FMA kernel), 0 = multiply then
+ * add (its generic kernel, hosts without FMA).  Process-wide. */
+void oracle_set_dot_fma(int32_t on);
+
 /* ndarray `a.dot(&b)` (row-major m x k times k x n) in the reference's product
  * order: sequential fused multiply-adds over k. */
 int oracle_dot(int64_t m, int64_t k, int64_t n, const double* A, const double* B, double* C);

@@ -288,6 +288,13 @@ class metrics:  # noqa: N801 -- mirrors the Rust module name
                           None if sigma_ref is None else out[4])
 
 
+def set_dot_fma(on: bool) -> None:
+    """Product rounding of the oracle's ndarray ``dot`` restatements: fused
+    multiply-add per k (matrixmultiply's FMA kernel, the default) or multiply
+    then add (its generic kernel on hosts without FMA).  Process-wide."""
+    lib().oracle_set_dot_fma(C.c_int32(1 if on else 0))
+
+
 def dot(a, b) -> np.ndarray:
     """ndarray ``a.dot(&b)`` in the reference's product order (sequential
     fused multiply-adds over k, matrixmultiply 0.3.11's f64 kernel)."""

@@ -7,6 +7,9 @@ into ``reference_outputs.json``:
   orth_v (README.md "Docker N=64 Smoke");
 * ``stress_cpu 32 --auto-trace`` rows of the same profiles (Auto -> Small):
   rel_recon (README.md "Adaptive N=32 Smoke");
+* ``compare/`` harness (run under ``--platform linux/amd64``, a host whose
+  matrixmultiply kernel has no FMA): ``LieSvdSmall::solve`` orth_u and
+  rel_recon of the named matrices (compare/README.md "Measured results");
 * ``stress_cpu --joint`` Phase-JADE smoke (family built by
   ``print_joint_phase_jade_smoke``, src/bin/stress_cpu.rs:472-500) and
   ``--joint-svd`` smoke (``print_joint_svd_smoke``, :597-624).
@@ -49,6 +52,19 @@ def main(ref_root: str) -> None:
                    "sweeps": int(m[5]), "rotations": int(m[6]), "readme_line": no}
             prev = "\n".join(lines[max(0, no - 12):no])
             out["joint_svd" if "Joint SVD Offdiag" in prev else "jade"].append(row)
+    out["compare_named"] = []
+    names = {"Kahan": "kahan", "Pei (`alpha=0.01`)": "pei", "Vandermonde": "vandermonde", "Hilbert": "hilbert"}
+    clines = open(os.path.join(ref_root, "compare", "README.md"), encoding="utf-8").read().splitlines()
+    for no, line in enumerate(clines, 1):
+        cells = [c.strip() for c in line.strip().strip("|").split("|")] if line.startswith("|") else []
+        if len(cells) == 5 and cells[0] in names:
+            out["compare_named"].append({"matrix": names[cells[0]], "n": int(cells[1]),
+                                         "orth_u": cells[2].split("/")[0].strip(),
+                                         "rel_recon": cells[3].split("/")[0].strip(),
+                                         "compare_readme_line": no})
+    assert len(out["compare_named"]) == 6, out["compare_named"]
+    m = re.search(r"max relative error vs exact closed form = ([0-9.e-]+)`\s+at\s+`n=(\d+)`", "\n".join(clines))
+    out["compare_pei_closed_form"] = {"n": int(m[2]), "alpha": 0.01, "max_rel": m[1]}
     assert len(out["small_n64"]) == 3 and len(out["auto_n32"]) == 3, out
     assert len(out["jade"]) == 4 and len(out["joint_svd"]) == 2, out
     with open(os.path.join(HERE, "reference_outputs.json"), "w") as f:

@@ -86,3 +86,40 @@ def test_joint_svd_smoke_n64():
     assert rust_e3(tr.initial_offdiag) == row["initial_offdiag"]
     assert (tr.sweeps, tr.rotations) == (row["sweeps"], row["rotations"])
     assert abs(tr.final_offdiag / float(row["final_offdiag"]) - 1) < 1e-3
+
+
+NAMED = {"kahan": lambda n: P.kahan_matrix(n, 1.2), "pei": lambda n: P.pei_matrix(n, 0.01),
+         "vandermonde": P.vandermonde_matrix, "hilbert": P.hilbert_matrix}
+
+
+def rust_e1(x: float) -> str:
+    m, e = f"{x:.1e}".split("e")
+    return f"{m}e{int(e)}"
+
+
+@pytest.mark.parametrize("row", GOLD["compare_named"], ids=lambda r: f"{r['matrix']}{r['n']}")
+def test_named_matrices_on_a_host_without_fma(row):
+    # the compare harness (compare/src/main.rs:36-57, matrices of src/lie_svd_benchmarks.rs) ran
+    # where matrixmultiply has no FMA kernel: the oracle's multiply-then-add products reproduce it
+    O.set_dot_fma(False)
+    try:
+        a = NAMED[row["matrix"]](row["n"])
+        u, s, vt = O.LieSvdSmall.solve(a)
+        m = O.metrics.compute(a, u, s, vt, None)
+    finally:
+        O.set_dot_fma(True)
+    assert (rust_e1(m.orth_u), rust_e1(m.rel_recon)) == (row["orth_u"], row["rel_recon"])
+
+
+def test_pei_closed_form_error_on_a_host_without_fma():
+    # compare/src/main.rs:173-186: max relative error of LieSvdSmall's sigma against the
+    # Pei closed form (n = 64, alpha = 0.01), printed as 1.0e-12
+    row = GOLD["compare_pei_closed_form"]
+    O.set_dot_fma(False)
+    try:
+        _, s, _ = O.LieSvdSmall.solve(P.pei_matrix(row["n"], row["alpha"]))
+    finally:
+        O.set_dot_fma(True)
+    want = np.sort(P.pei_matrix_singular_values(row["n"], row["alpha"]))[::-1]
+    got = np.sort(s)[::-1]
+    assert rust_e1(float(np.max(np.abs(got - want) / np.maximum(np.abs(want), 1e-300)))) == row["max_rel"]
