@@ -95,13 +95,15 @@ def cpu_cores() -> int:
 
 
 def flops_per_matrix(n, ns_iters, sweeps, rotations, route):
-    """Executed FP64 flops of one solve.  Small route: Newton-Schulz
-    iterations x (X^T X + X T) + final X^T X, P = Q^T A, U = Q V, U^T U,
-    plus per Jacobi sweep n(n-1)/2 pairs x 3 dot products (6n) and per
-    accepted rotation the update of two columns of W and V (12n).
-    Micro route: per rotation 4 two-row/column updates (~24n)."""
+    """FP64 flops of one solve by the reference algorithm (the algorithmic
+    count the roofline uses).  Small route: Newton-Schulz iterations x
+    (X^T X + X T), the final X^T X, P = Q^T A, U = Q V and U^T U, each 2n^3
+    (src/lie_svd_small.rs:158-183, :296-323); per Jacobi sweep the off-norm
+    test, n(n-1) (:220-228); per accepted rotation the update of two rows and
+    columns of P and two columns of V, 12n (:244-270).  Micro route: per
+    rotation 4 two-row/column updates (~24n)."""
     n = n.astype(np.float64)
-    small = (4.0 * ns_iters + 8.0) * n ** 3 + sweeps * n * (n - 1) / 2 * 6 * n + rotations * 12 * n
+    small = (4.0 * ns_iters + 8.0) * n ** 3 + sweeps * n * (n - 1) + rotations * 12 * n
     micro = rotations * 24.0 * n + 2 * n ** 3
     return np.where(route == 0, micro, small)
 

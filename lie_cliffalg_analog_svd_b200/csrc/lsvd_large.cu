@@ -16,7 +16,7 @@
 // reference's start-of-sweep test off(P) < 1e-13 ||P||_F (offnorm_part_kernel, offnorm_final_kernel);
 // per layer
 //   solve2_kernel   diagonalises the 64 x 64 diagonal block of every block
-//                   pair by cyclic Jacobi sweeps (Rutishauser tangent,
+//                   pair by cyclic Jacobi sweeps (the reference's tangent,
 //                   parallel round-robin order) into one orthogonal R
 //   twoside_kernel  P <- R^T P R, one CTA per 64 x 64 block of the
 //                   block-pair triangle (R_a^T P_ab R_b)
@@ -313,11 +313,15 @@ __device__ int pair_rounds(double* Ms, bool with_inner, int inner_max, Rot rotat
                 double c = 1.0, s = 0.0;
                 const bool rot = apq != 0.0 && rotate(app, aqq, apq);
                 if (rot) {
-                    const double zeta = (aqq - app) / (2.0 * apq);
-                    const double t = fabs(zeta) > 1e150
-                                         ? 0.5 / zeta
-                                         : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    c = rsqrt(1.0 + t * t);
+                    // the reference's smaller-root tangent (src/lie_svd_small.rs:235-242, its
+                    // theta >= 0 branch for theta = -0 included); the cosine by one reciprocal
+                    // square root: each column of V takes tens of thousands of rotations
+                    // here, and 1 / sqrt(.) with its two roundings leaves c^2 + s^2 biased
+                    // enough that the orthogonality drifts (10-20x larger at n = 2048)
+                    const double theta = (aqq - app) / (2.0 * apq);
+                    const double t = theta >= 0.0 ? 1.0 / (theta + sqrt(theta * theta + 1.0))
+                                                  : -1.0 / (-theta + sqrt(theta * theta + 1.0));
+                    c = rsqrt(t * t + 1.0);
                     s = t * c;
                 }
                 const unsigned msk = __ballot_sync(0xffffffffu, rot);
@@ -401,8 +405,8 @@ __device__ int pair_rounds(double* Ms, bool with_inner, int inner_max, Rot rotat
 // Two-sided route (1024 threads: the rounds of a block-pair solve are the
 // critical path of every layer): gathers the 64 x 64 diagonal block M of
 // block pair blockIdx.x from P, rotates (|a_pq| > tau; the reference rotates
-// every |a_pq| >= 1e-300, src/lie_svd_small.rs:233-235, with the Rutishauser
-// tangent, :235-242) and writes R / skip like solve_kernel.  Every index pair
+// every |a_pq| >= 1e-300, src/lie_svd_small.rs:233-235, with the smaller-root
+// tangent of :235-242) and writes R / skip like solve_kernel.  Every index pair
 // is visited once per sweep, as in the reference: its 32 cross rounds
 // (lo x hi pairs) on every layer, the 31 inner rounds of both blocks on
 // layer 0 only (every block is in a layer-0 pair).  Per round, warp 0
@@ -445,8 +449,8 @@ __global__ void __launch_bounds__(1024) solve2_kernel(const double* __restrict__
     double l0, l1, h0, h1;
     int cnt = 0;
     const int sw = pair_rounds(
-        Ms, with_inner, inner_max, [&](double, double, double apq) { return fabs(apq) > tau; }, cs, sn, &s_flag, cnt,
-        l0, l1, h0, h1);
+        Ms, with_inner, inner_max, [&](double, double, double apq) { return fabs(apq) > tau; }, cs, sn, &s_flag,
+        cnt, l0, l1, h0, h1);
     double* R = Rg + int64_t(pair) * (PW * PW);
     R[warp * PW + lane] = l0;
     R[warp * PW + BW + lane] = h0;
