@@ -786,14 +786,17 @@ extern "C" lsvd_status lsvd_class_shapes(lsvd_context* ctx, lsvd_precision preci
 }
 
 // Host-pointer batches of at least kPipeMin matrices are cut into kPipeChunks
-// contiguous chunks of equal cost (sum of n^3), each with its own plan and
-// staging buffers (its own slot, even when two chunks have equal size lists),
-// so that the copies overlap the solves: H2D of every chunk
-// on one copy stream, the solves in order on the context stream, D2H of
-// chunk c on a second copy stream as soon as its solve is done.  The results
-// are those of the unchunked call (every matrix is solved independently).
+// contiguous chunks, each with its own plan and staging buffers (its own slot,
+// even when two chunks have equal size lists), so that the copies overlap the
+// solves: H2D of every chunk on one copy stream, the solves in order on the
+// context stream, D2H of chunk c on a second copy stream as soon as its solve
+// is done.  Only the first chunk's H2D and the last chunk's D2H stay exposed,
+// so the chunk costs (sum of n^3) ramp up and down, kPipeWeight / 20 of the
+// total each.  The results are those of the unchunked call (every matrix is
+// solved independently).
 constexpr int64_t kPipeMin = 16384;
-constexpr int kPipeChunks = 4;
+constexpr int kPipeChunks = 8;
+constexpr int kPipeWeight[kPipeChunks] = {1, 2, 3, 4, 4, 3, 2, 1};
 
 static lsvd_status batched_pipelined(lsvd_context* ctx, int64_t count, const int32_t* n, const double* A,
                                      double* U, double* S, double* Vt, lsvd_diag* diags,
@@ -809,8 +812,11 @@ static lsvd_status batched_pipelined(lsvd_context* ctx, int64_t count, const int
     for (int64_t t = 0; t < count; ++t) pre[t + 1] = pre[t] + double(n[t]) * n[t] * n[t];
     int64_t cut[C + 1];
     cut[0] = 0;
+    int wsum = 0, wtot = 0;
+    for (int c = 0; c < C; ++c) wtot += kPipeWeight[c];
     for (int c = 1; c < C; ++c) {
-        const int64_t x = std::lower_bound(pre.begin(), pre.end(), pre[count] * c / C) - pre.begin();
+        wsum += kPipeWeight[c - 1];
+        const int64_t x = std::lower_bound(pre.begin(), pre.end(), pre[count] * wsum / wtot) - pre.begin();
         cut[c] = std::min(std::max(x, cut[c - 1] + 1), count - (C - c));
     }
     cut[C] = count;

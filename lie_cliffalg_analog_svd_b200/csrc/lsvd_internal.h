@@ -94,7 +94,7 @@ struct lsvd_context {
     std::unordered_map<uint64_t, std::unique_ptr<BatchPlan>> plans;
     // one plan per chunk of the pipelined host-pointer path: every chunk owns
     // its staging buffers, even when two chunks have the same size list
-    std::unique_ptr<BatchPlan> pipe_plans[4];
+    std::unique_ptr<BatchPlan> pipe_plans[8];
     void* pinned = nullptr;  // small page-locked host buffer (device-to-host status reads)
     size_t pinned_bytes = 0;
     ~lsvd_context();
