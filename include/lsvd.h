@@ -42,7 +42,7 @@ typedef enum lsvd_status {
     LSVD_OUT_OF_MEMORY = 6,
     LSVD_ROTOR_OVERFLOW = 7,  /* rotor buffer too small; count holds the need */
     LSVD_NO_DEVICE = 8,
-    LSVD_UNSUPPORTED = 9      /* size or option outside what this build handles */
+    LSVD_UNSUPPORTED = 9      /* size or option outside what the library supports */
 } lsvd_status;
 
 /* flags */

@@ -2,9 +2,8 @@
 
 TEST INFRASTRUCTURE ONLY.  The oracle is a C++ f64 restatement of the Rust
 crate ``lie_cliffalg_analog_svd`` v0.44.0 hot path (see ``lsvd_oracle.cpp``
-for the file:line each routine follows).  Only ``tests/``,
-``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline legs import this
-module, always as the checker or the timed CPU baseline -- never as the
+for the file:line each routine follows).  Only ``tests/``, the smoke
+entry point and ``bench.py``'s CPU-baseline legs import this module, always as the checker or the timed CPU baseline -- never as the
 product path.
 
 The names mirror the reference API: ``LieSvdSmall.solve``,
