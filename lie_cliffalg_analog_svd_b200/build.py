@@ -1,6 +1,6 @@
 """Builds ``liblsvd_b200.so`` (the C ABI of ``include/lsvd.h``) in-tree with
 nvcc for sm_100a.  Objects are cached under ``_build/`` next to this file and
-rebuilt when a source or header is newer.
+rebuilt when their source, a header or the flags changed (content digests).
 
     python -m lie_cliffalg_analog_svd_b200.build [--force] [--verbose]
 """
@@ -9,6 +9,7 @@ from __future__ import annotations
 import argparse
 import concurrent.futures as cf
 import glob
+import hashlib
 import os
 import shutil
 import subprocess
@@ -34,23 +35,32 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _deps_mtime() -> float:
-    files = glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(INCLUDE, "*.h"))
-    return max(os.path.getmtime(f) for f in files)
+def _headers_digest() -> str:
+    h = hashlib.sha256()
+    for f in sorted(glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+                    glob.glob(os.path.join(INCLUDE, "*.h"))):
+        h.update(f.encode())
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()
 
 
-def _headers_mtime() -> float:
-    files = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
-        glob.glob(os.path.join(INCLUDE, "*.h"))
-    return max(os.path.getmtime(f) for f in files)
-
-
-def _compile(src: str, verbose: bool, extra: list[str], reuse_after: float | None = None) -> str:
+def _compile(src: str, verbose: bool, extra: list[str], headers: str, reuse: bool) -> str:
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    # an object newer than its source and every header is current
-    if reuse_after is not None and os.path.exists(obj) and \
-            os.path.getmtime(obj) >= max(os.path.getmtime(src), reuse_after):
-        return obj
+    # an object is current when it was built from this source, these headers and
+    # these flags (content, not timestamps: an edit made while a build runs must
+    # not leave an object compiled from the old text looking fresh)
+    h = hashlib.sha256()
+    with open(src, "rb") as fh:
+        h.update(fh.read())
+    h.update(headers.encode())
+    h.update(" ".join([*ARCH, *NVCC_FLAGS, *extra]).encode())
+    sig = h.hexdigest()
+    sig_path = obj + ".sig"
+    if reuse and os.path.exists(obj) and os.path.exists(sig_path):
+        with open(sig_path) as fh:
+            if fh.read().strip() == sig:
+                return obj
     cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", src, "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
@@ -59,6 +69,8 @@ def _compile(src: str, verbose: bool, extra: list[str], reuse_after: float | Non
         raise RuntimeError(f"nvcc failed on {os.path.basename(src)}:\n{r.stdout}\n{r.stderr}")
     if verbose and (r.stdout or r.stderr):
         print(r.stdout, r.stderr, flush=True)
+    with open(sig_path, "w") as fh:
+        fh.write(sig)
     return obj
 
 
@@ -68,12 +80,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _deps_mtime():
-        return LIB
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        reuse = None if (force or ptxas_verbose) else _headers_mtime()
-        objs = list(ex.map(lambda s: _compile(s, verbose or ptxas_verbose, extra, reuse), srcs))
+        headers, reuse = _headers_digest(), not (force or ptxas_verbose)
+        objs = list(ex.map(lambda s: _compile(s, verbose or ptxas_verbose, extra, headers, reuse), srcs))
+    # relink only when an object is newer than the library (freshness is decided per
+    # object against its source and the headers, so an edit made while another build
+    # ran is never masked by that build's library)
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
+        return LIB
     cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

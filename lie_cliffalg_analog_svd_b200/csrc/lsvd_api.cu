@@ -120,6 +120,7 @@ lsvd_context::~lsvd_context() {
     if (pinned) cudaFreeHost(pinned);
     if (h2d_stream) cudaStreamDestroy(h2d_stream);
     if (side_stream) cudaStreamDestroy(side_stream);
+    if (side_stream2) cudaStreamDestroy(side_stream2);
     if (d2h_stream) cudaStreamDestroy(d2h_stream);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }

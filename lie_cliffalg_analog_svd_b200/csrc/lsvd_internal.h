@@ -91,6 +91,7 @@ struct lsvd_context {
     cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
     // side branch of the large solve's sweep graph (V's update), created on first use
     cudaStream_t side_stream = nullptr;
+    cudaStream_t side_stream2 = nullptr;  // large solve: the P update tiles the next layer does not read
     std::unordered_map<uint64_t, std::unique_ptr<BatchPlan>> plans;
     // one plan per chunk of the pipelined host-pointer path: every chunk owns
     // its staging buffers, even when two chunks have the same size list

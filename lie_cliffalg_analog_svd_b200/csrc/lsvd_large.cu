@@ -527,19 +527,28 @@ __global__ void __launch_bounds__(1024) solve_kernel(const double* __restrict__ 
 // pairs a and b (R = I for a skipped pair) and writes C to P_ab and C^T to
 // P_ba; the blocks are disjoint, so every block of P is written once.
 // Both products on the FP64 tensor path.
+// tiles: NULL for every block pair (a, b) of the triangle (CTA i = the i-th
+// in row order), else CTA i takes tile tiles[i] = a * 65536 + b.
 __global__ void __launch_bounds__(256, 2) twoside_kernel(double* __restrict__ P, int64_t ldp, int nb, int layer,
                                                          const double* __restrict__ Rg,
                                                          const int* __restrict__ skip,
-                                                         const SweepState* __restrict__ stt) {
+                                                         const SweepState* __restrict__ stt,
+                                                         const int* __restrict__ tiles) {
     if (stt->converged) return;
-    // (a, b) from the linear CTA index over the upper triangle of npairs x npairs
-    const int npairs = nb / 2;
-    int a = 0, rem = blockIdx.x;
-    while (rem >= npairs - a) {
-        rem -= npairs - a;
-        ++a;
+    int a = 0, b = 0;
+    if (tiles) {
+        a = tiles[blockIdx.x] >> 16;
+        b = tiles[blockIdx.x] & 0xffff;
+    } else {
+        // (a, b) from the linear CTA index over the upper triangle of npairs x npairs
+        const int npairs = nb / 2;
+        int rem = blockIdx.x;
+        while (rem >= npairs - a) {
+            rem -= npairs - a;
+            ++a;
+        }
+        b = a + rem;
     }
-    const int b = a + rem;
     const bool ra = !skip[a], rb = !skip[b];
     if (!ra && !rb) return;
     extern __shared__ __align__(16) double tsm[];
@@ -1064,6 +1073,58 @@ static lsvd_status run_sweeps(lsvd_context* ctx, double* H, int64_t ldh, int gm,
 // reference's start-of-sweep test off(P) < limit (offnorm_part_kernel, offnorm_final_kernel), then for
 // every round-robin layer the block solves (solve2_kernel), P <- R^T P R
 // (twoside_kernel) and V <- V R (apply_kernel on Vc).
+// Host twin of block_pair.
+static void block_pair_host(int nb, int layer, int k, int& a, int& b) {
+    const int ring = nb - 1;
+    if (k == 0) {
+        a = nb - 1;
+        b = layer % ring;
+    } else {
+        a = (layer + k) % ring;
+        b = (layer + ring - k) % ring;
+    }
+}
+
+// The twoside tiles (a <= b, a * 65536 + b) of every layer of a sweep, split
+// for the next layer's solves: first the n1[L] tiles that hold the next
+// layer's diagonal block-pair blocks -- tile (x, x) and (y, y) and the one
+// between them, x, y the layer-L pairs of the next pair's two blocks -- then
+// the rest, which can run beside the next layer's solves.  The last layer of
+// a sweep has no next layer in the sweep: all its tiles come first.
+static void twoside_tiles(int nb, std::vector<int>& tiles, std::vector<int>& n1) {
+    const int npairs = nb / 2, ntri = npairs * (npairs + 1) / 2, layers = nb - 1;
+    tiles.assign(size_t(layers) * ntri, 0);
+    n1.assign(size_t(layers), ntri);
+    std::vector<int> pof(size_t(nb), 0);
+    std::vector<char> need(size_t(npairs) * npairs);
+    for (int L = 0; L < layers; ++L) {
+        for (int k = 0; k < npairs; ++k) {
+            int a, b;
+            block_pair_host(nb, L, k, a, b);
+            pof[size_t(a)] = pof[size_t(b)] = k;
+        }
+        std::fill(need.begin(), need.end(), char(L + 1 == layers));
+        if (L + 1 < layers)
+            for (int k = 0; k < npairs; ++k) {
+                int a, b;
+                block_pair_host(nb, L + 1, k, a, b);
+                const int x = pof[size_t(a)], y = pof[size_t(b)];
+                need[size_t(x) * npairs + x] = need[size_t(y) * npairs + y] = 1;
+                need[size_t(std::min(x, y)) * npairs + std::max(x, y)] = 1;
+            }
+        int* t = tiles.data() + size_t(L) * ntri;
+        int c = 0;
+        for (int pass = 0; pass < 2; ++pass)
+            for (int a = 0; a < npairs; ++a)
+                for (int b = a; b < npairs; ++b)
+                    if ((need[size_t(a) * npairs + b] != 0) == (pass == 0)) t[c++] = a * 65536 + b;
+        int first = 0;
+        for (int a = 0; a < npairs; ++a)
+            for (int b = a; b < npairs; ++b) first += need[size_t(a) * npairs + b] != 0;
+        n1[size_t(L)] = first;
+    }
+}
+
 static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, int npad, double limit, double tau,
                                int max_sweeps, int inner_max, char* ws, int* sweeps_out, int64_t* rot_out,
                                double* off_out, int* inner_cap_out, double* ms_out) {
@@ -1087,15 +1148,23 @@ static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, 
     Rg2[0] = reinterpret_cast<double*>(p); p += al(size_t(npairs) * PW * PW * 8);
     Rg2[1] = reinterpret_cast<double*>(p); p += al(size_t(npairs) * PW * PW * 8);
     double* offpart = reinterpret_cast<double*>(p);  // 256 partial sums of the off-norm test
-    cudaError_t e = cudaMemsetAsync(stt, 0, sizeof(SweepState), st);
+    p += al(256 * 8);
+    // twoside's tile lists per layer
+    int* tiles_d = reinterpret_cast<int*>(p);
+    std::vector<int> tiles_h, n1;
+    twoside_tiles(nb, tiles_h, n1);
+    cudaError_t e = cudaMemcpy(tiles_d, tiles_h.data(), tiles_h.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemsetAsync(stt, 0, sizeof(SweepState), st);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(solve2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolve2Smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(twoside_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTwoSmem);
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: sweep setup");
     if (!ctx->side_stream && (e = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking)) != cudaSuccess)
         return lsvd_ctx_cuda(ctx, e, "large: side stream");
-    cudaStream_t sv = ctx->side_stream;
-    cudaEvent_t evs[4] = {nullptr, nullptr, nullptr, nullptr};  // fork, join, applied[2]
+    if (!ctx->side_stream2 && (e = cudaStreamCreateWithFlags(&ctx->side_stream2, cudaStreamNonBlocking)) != cudaSuccess)
+        return lsvd_ctx_cuda(ctx, e, "large: side stream");
+    cudaStream_t sv = ctx->side_stream, s2 = ctx->side_stream2;
+    cudaEvent_t evs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // solved, join, applied[2], rest done
     for (auto& x : evs)
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
     auto destroy_events = [&]() {
@@ -1114,17 +1183,33 @@ static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, 
     }
     offnorm_part_kernel<<<256, 256, 0, st>>>(P, npad, n, stt, offpart);
     offnorm_final_kernel<<<1, 256, 0, st>>>(offpart, 256, stt, limit);
+    // Per layer L: solve2(L); V <- V R on sv; P <- R^T P R split in two: the tiles the
+    // next layer's solves read, on st, and the rest on s2, beside solve2(L + 1).  The
+    // rest of layer L - 1 finishes before any tile of layer L starts (a tile of L
+    // reads blocks that tiles of L - 1 wrote); R / skip of parity b are rewritten by
+    // solve2(L + 2) only after V's update of L (applied[b]) and the rest of L (which
+    // precedes the first part of L + 1 on st).
+    bool rest_pending = false;  // the previous layer left tiles on s2
     for (int layer = 0; layer < nb - 1; ++layer) {
         const int b = layer & 1;
-        // the buffers of parity b were last read by V's update two layers back
+        const int* tl = tiles_d + size_t(layer) * ntri;
+        const int k1 = n1[size_t(layer)];
         if (layer >= 2) cudaStreamWaitEvent(st, evs[2 + b], 0);
         solve2_kernel<<<npairs, 1024, kSolve2Smem, st>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt, tau, inner_max);
         cudaEventRecord(evs[0], st);
         cudaStreamWaitEvent(sv, evs[0], 0);
         apply_kernel<<<dim3(npairs, napply), 256, kApplySmem, sv>>>(Vc, npad, nb, layer, rows, Rg2[b], skip2[b], stt);
         cudaEventRecord(evs[2 + b], sv);
-        twoside_kernel<<<ntri, 256, kTwoSmem, st>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt);
+        if (rest_pending) cudaStreamWaitEvent(st, evs[4], 0);  // the rest of layer - 1
+        twoside_kernel<<<k1, 256, kTwoSmem, st>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt, tl);
+        rest_pending = k1 < ntri;
+        if (rest_pending) {
+            cudaStreamWaitEvent(s2, evs[0], 0);
+            twoside_kernel<<<ntri - k1, 256, kTwoSmem, s2>>>(P, npad, nb, layer, Rg2[b], skip2[b], stt, tl + k1);
+            cudaEventRecord(evs[4], s2);
+        }
     }
+    if (rest_pending) cudaStreamWaitEvent(st, evs[4], 0);
     cudaEventRecord(evs[1], sv);
     cudaStreamWaitEvent(st, evs[1], 0);
     sweep_end_kernel<<<1, 1, 0, st>>>(stt, -1.0);
@@ -1138,7 +1223,8 @@ static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, 
     e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "large: graph instantiate");
-    const int launches_per_sweep = 3 * (nb - 1) + 3;
+    int launches_per_sweep = 3;  // off-norm test, its final step, sweep end
+    for (int L = 0; L < nb - 1; ++L) launches_per_sweep += 3 + (n1[size_t(L)] < ntri ? 1 : 0);
     SweepState* hst = static_cast<SweepState*>(lsvd_ctx_pinned(ctx, 2 * sizeof(SweepState)));
     cudaEvent_t ev[2] = {nullptr, nullptr};
     lsvd_status out = LSVD_OK;
@@ -1195,8 +1281,10 @@ static size_t sweep_ws_bytes(int gpad, int npad, int num_sms) {
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     // state | skip x 2 | rotations x 2 | Gram partials (the two-sided route uses the second
     // skip and rotation buffers, the one-sided route the partials)
+    // | twoside's tile lists per layer (the two-sided route)
+    const size_t ntri = size_t(npairs) * (npairs + 1) / 2;
     return al(sizeof(SweepState)) + 2 * al(size_t(npairs) * 4) + 2 * al(size_t(npairs) * PW * PW * 8) +
-           al(256 * 8) + al(size_t(npairs) * (nchunk + 1) * PW * PW * 8);
+           al(256 * 8) + al(size_t(npairs) * (nchunk + 1) * PW * PW * 8) + al(size_t(nb - 1) * ntri * 4);
 }
 
 static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,
