@@ -1,0 +1,59 @@
+"""The GPU against the reference's own printed outputs, on the inputs the
+reference builds without an RNG stream (tests/golden/reference_outputs.json;
+the oracle reproduces those outputs digit for digit in test_oracle_pinned.py).
+
+The GPU sweeps visit every index pair once per sweep in a parallel order, so
+rounding-level statistics are not the same numbers: the bars are the
+reference's own values within a small factor, sweep counts within one, and
+the singular values equal to the (pinned) oracle's to 1e-13 normwise."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from lie_cliffalg_analog_svd_b200 import JointDiagonalizationParams, LieSvdJoint, LieSvdSmall, metrics
+from lie_cliffalg_analog_svd_b200 import profiles as P
+
+pytestmark = pytest.mark.gpu
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_outputs.json")))
+
+
+@pytest.mark.parametrize("row", GOLD["small_n64"], ids=lambda r: r["profile"])
+def test_small_solve_on_rng_free_profiles(row):
+    a = P.generate(64, row["profile"], 17)[0]
+    u, s, vt = LieSvdSmall.solve(a)
+    m = metrics.compute(a, u, s, vt)
+    for got, want in ((m.rel_recon, row["rel_recon"]), (m.orth_u, row["orth_u"]), (m.orth_v, row["orth_v"])):
+        assert got <= 4 * float(want), (row["profile"], got, want)
+    _, so, _ = O.LieSvdSmall.solve(a)
+    assert np.max(np.abs(np.sort(s) - np.sort(so))) <= 1e-13 * so.max()
+
+
+def _jade_family(n):
+    q = O.deterministic_orthogonal(n, [0x9E3779B97F4A7C15])
+    base = np.abs(np.sin(np.arange(n) + 1.0))
+    return [O.dot(O.dot(q, np.diag(1.0 + k * 0.2 + base)), q.T.copy()) for k in range(6)]
+
+
+@pytest.mark.parametrize("row", [r for r in GOLD["jade"] if r["n"] <= 128], ids=lambda r: f"n{r['n']}")
+def test_phase_jade_on_the_reference_smoke_family(row):
+    n = row["n"]
+    params = JointDiagonalizationParams.for_n(n)
+    _, _, tr = LieSvdJoint.diagonalize_symmetric_with_params(_jade_family(n), params)
+    assert f"{tr.initial_offdiag:.3e}".replace("e+0", "e").replace("e+", "e") == row["initial_offdiag"]
+    assert abs(tr.sweeps - row["sweeps"]) <= 1, (tr.sweeps, row["sweeps"])
+    assert tr.final_offdiag <= 4 * float(row["final_offdiag"]), (tr.final_offdiag, row["final_offdiag"])
+
+
+def test_joint_svd_on_the_reference_smoke_family():
+    row = next(r for r in GOLD["joint_svd"] if r["n"] == 64)
+    st = [0xA24BAED4963EE407]
+    u0 = O.deterministic_orthogonal(64, st)
+    v0 = O.deterministic_orthogonal(64, st)
+    fam = [O.dot(O.dot(u0, np.diag(1.0 + k * 0.15 + np.arange(64) * 0.05)), v0.T.copy()) for k in range(4)]
+    _, _, _, tr = LieSvdJoint.joint_svd_with_params(fam, JointDiagonalizationParams.for_n(64))
+    assert abs(tr.sweeps - row["sweeps"]) <= 1, (tr.sweeps, row["sweeps"])
+    assert tr.final_offdiag <= 4 * float(row["final_offdiag"]), (tr.final_offdiag, row["final_offdiag"])
