@@ -55,5 +55,7 @@ def test_joint_svd_on_the_reference_smoke_family():
     v0 = O.deterministic_orthogonal(64, st)
     fam = [O.dot(O.dot(u0, np.diag(1.0 + k * 0.15 + np.arange(64) * 0.05)), v0.T.copy()) for k in range(4)]
     _, _, _, tr = LieSvdJoint.joint_svd_with_params(fam, JointDiagonalizationParams.for_n(64))
-    assert abs(tr.sweeps - row["sweeps"]) <= 1, (tr.sweeps, row["sweeps"])
+    # the blocked order with separate left/right block rotations converges in fewer
+    # sweeps here (9 against the reference's 12): never more than one above it
+    assert tr.sweeps <= row["sweeps"] + 1, (tr.sweeps, row["sweeps"])
     assert tr.final_offdiag <= 4 * float(row["final_offdiag"]), (tr.final_offdiag, row["final_offdiag"])
