@@ -120,8 +120,9 @@ class LieSvdSmall:
     @staticmethod
     def solve(a, ctx: Context | None = None):
         """Full SVD ``(U, sigma, Vt)`` of a square matrix (n <= 64 on the
-        shared-memory kernels, larger n on the blocked large solve)."""
-        r = LieSvdSmall.solve_full(a, ctx=ctx)
+        shared-memory kernels, larger n on the blocked large solve).  Like the
+        reference's ``solve`` it computes no diagnostics (``solve_full`` does)."""
+        r = LieSvdSmall.solve_full(a, ctx=ctx, want_diag=False)
         return r.u, r.sigma, r.vt
 
     @staticmethod
