@@ -39,11 +39,15 @@
 
 #include "lsvd.h"
 #include "lsvd_internal.h"
+#include "lsvd_dgemm.cuh"
 #include "lsvd_joint_common.cuh"
 
 namespace {
 
 using namespace lsvd::joint;
+using lsvd::dg::cp_async16;
+using lsvd::dg::cp_async_commit;
+using lsvd::dg::cp_async_wait;
 
 struct JadeArgs {
     int F, K, n, nbe;        // families, matrices per family, order, blocks (even)
@@ -56,6 +60,7 @@ struct JadeArgs {
     long long* rot;          // per family: accepted, rejected
     const int* active;       // per family
     double* part;            // last layer of a sweep: per matrix (offdiag^2, all^2), else null
+    int prefetch;            // apply: strips staged by cp.async one strip ahead (n even)
 };
 
 // Block pair (A, Bk) of `layer` -> the 16 global indices (B of block A, then
@@ -276,7 +281,11 @@ __global__ void __launch_bounds__(kThreads, 2) jade_apply_kernel(JadeArgs a) {
     double* M = isV ? a.V + size_t(f) * n * n : a.W + (size_t(f) * a.K + k) * n * n;
     double* Rall = ash;                              // nbp * B2 * B2
     double* T = Rall + size_t(nbp) * B2 * B2;        // B2 x ldt
-    int* blo = reinterpret_cast<int*>(T + size_t(B2) * ldt);
+    // with prefetch: the next strip's rows, row stride n + 2 (16-byte rows for cp.async)
+    const bool pre = a.prefetch != 0;
+    const int ldi = n + 2;
+    double* Tin = T + size_t(B2) * ldt;
+    int* blo = reinterpret_cast<int*>(Tin + (pre ? size_t(B2) * ldi : 0));
     int* bhi = blo + 32 * 4;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double sum_off = 0.0, sum_all = 0.0;
@@ -288,17 +297,42 @@ __global__ void __launch_bounds__(kThreads, 2) jade_apply_kernel(JadeArgs a) {
         blo[q] = min(A, Bb);
         bhi[q] = max(A, Bb);
     }
+    // strip P's 2B rows into Tin: 16-byte cp.async chunks (padding rows zeroed)
+    auto stage = [&](int P) {
+        const int pl = blo[P], ph = bhi[P], per_row = n / 2;
+        for (int c = tid; c < B2 * per_row; c += kThreads) {
+            const int r = c / per_row, ch = c - r * per_row;
+            const int g = block_pos(pl, ph, r, n);
+            double* dst = Tin + size_t(r) * ldi + 2 * ch;
+            if (g >= 0) {
+                cp_async16(dst, M + size_t(g) * n + 2 * ch, 16);
+            } else {
+                dst[0] = 0.0;
+                dst[1] = 0.0;
+            }
+        }
+        cp_async_commit();
+    };
     __syncthreads();
+    if (pre) stage(0);
     for (int P = 0; P < nbp; ++P) {
         const int plo = blo[P], phi = bhi[P];
         const double* RP = Rall + size_t(P) * B2 * B2;
+        if (pre) {
+            cp_async_wait<0>();
+            __syncthreads();  // strip P is in Tin for every thread
+        }
         // ---- load + left multiply (V: plain copy)
         for (int col = tid; col < n; col += kThreads) {
             double x[B2];
 #pragma unroll
             for (int r = 0; r < B2; ++r) {
-                const int g = block_pos(plo, phi, r, n);
-                x[r] = g >= 0 ? M[size_t(g) * n + col] : 0.0;
+                if (pre) {
+                    x[r] = Tin[r * ldi + col];
+                } else {
+                    const int g = block_pos(plo, phi, r, n);
+                    x[r] = g >= 0 ? M[size_t(g) * n + col] : 0.0;
+                }
             }
             if (isV) {
 #pragma unroll
@@ -319,6 +353,8 @@ __global__ void __launch_bounds__(kThreads, 2) jade_apply_kernel(JadeArgs a) {
             }
         }
         __syncthreads();
+        // every thread is done with Tin: fetch the next strip behind the right multiply and store
+        if (pre && P + 1 < nbp) stage(P + 1);
         // ---- right multiply by R_Q, in place in the strip
         {
             const int rr = lane % B, c0 = 4 * (lane / B);  // rows rr, rr + B; columns c0 .. c0 + 3
@@ -542,9 +578,13 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
                                   int(smem))) != cudaSuccess)
         return lsvd_ctx_cuda(ctx, e, "jade smem");
     // apply: all R of a family + one strip of 2B rows (row stride n + 1) + block tables
-    const size_t asmem = size_t(nbp) * B2 * B2 * 8 + size_t(B2) * (n + 1) * 8 + 2 * 32 * 4 * 4;
+    size_t asmem = size_t(nbp) * B2 * B2 * 8 + size_t(B2) * (n + 1) * 8 + 2 * 32 * 4 * 4;
     if (asmem > 200 * 1024)
         return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "LieSvdJoint: n too large for the apply pass");
+    // the prefetch buffer (next strip, row stride n + 2) where rows are 16-byte multiples and it fits
+    const size_t pre_bytes = size_t(B2) * (n + 2) * 8;
+    const bool prefetch = n % 2 == 0 && asmem + pre_bytes <= 100 * 1024;
+    if (prefetch) asmem += pre_bytes;
     if ((e = cudaFuncSetAttribute(jade_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(asmem))) != cudaSuccess)
         return lsvd_ctx_cuda(ctx, e, "jade apply smem");
@@ -554,6 +594,7 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
     a.n = int(n);
     a.nbe = nbe;
     a.steps = p.line_search_steps;
+    a.prefetch = prefetch ? 1 : 0;
     a.pair_tol = ptol;
     a.W = dW;
     a.V = dV;
