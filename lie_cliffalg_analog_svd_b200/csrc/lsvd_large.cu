@@ -742,23 +742,6 @@ __global__ void sweep_end_kernel(SweepState* stt, double tol_conv) {
     stt->next_scale2 = 0ull;
 }
 
-// H (column j = [g_j (gpad rows); v_j (npad rows)]) from the symmetric part of
-// P (n x n, ld) scaled by `scale`; V = I; padding zero.
-__global__ void fill_h_sym_kernel(const double* P, int64_t ld, int n, double scale, double* H, int64_t ldh,
-                                  int gpad, int npad) {
-    const int64_t tot = int64_t(npad) * ldh;
-    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < tot; e += int64_t(gridDim.x) * blockDim.x) {
-        const int j = int(e / ldh), r = int(e % ldh);
-        double v = 0.0;
-        if (r < gpad) {
-            if (j < n && r < n) v = 0.5 * scale * (P[int64_t(r) * ld + j] + P[int64_t(j) * ld + r]);
-        } else {
-            v = (r - gpad) == j ? 1.0 : 0.0;
-        }
-        H[e] = v;
-    }
-}
-
 // P2 (npad x npad) = scale sym(P) with zero padding; Vc (npad x npad) = I.
 __global__ void fill_p2v_kernel(const double* P, int64_t ld, int n, double scale, double* P2, double* Vc, int npad) {
     const int64_t tot = int64_t(npad) * npad;
