@@ -311,3 +311,75 @@ pub fn svd_large(mat: &Array2<f64>, precision: Precision) -> (Svd, LsvdLargeInfo
     });
     ((u, s, vt), info)
 }
+
+/// The reference's `HardwareTarget` (src/lie_svd_compiler.rs:12-25).
+#[derive(Clone, Copy, Debug, PartialEq, Eq)]
+pub enum HardwareTarget {
+    MziMesh,
+    FpgaRotorMesh,
+}
+
+impl HardwareTarget {
+    fn code(self) -> i32 {
+        match self {
+            HardwareTarget::MziMesh => 0,
+            HardwareTarget::FpgaRotorMesh => 1,
+        }
+    }
+}
+
+fn text_call(what: &str, f: impl Fn(*mut std::os::raw::c_char, i64, *mut i64) -> Status) -> String {
+    let mut len = 0i64;
+    let st = f(std::ptr::null_mut(), 0, &mut len);
+    assert_eq!(st, LSVD_OK, "{what} sizing failed: {}", status_text(st));
+    let mut buf = vec![0u8; len as usize + 1];
+    let st = f(buf.as_mut_ptr() as *mut std::os::raw::c_char, len + 1, &mut len);
+    assert_eq!(st, LSVD_OK, "{what} failed: {}", status_text(st));
+    buf.truncate(len as usize);
+    String::from_utf8(buf).expect("phase-schedule-v1 text is ASCII")
+}
+
+/// `HardwareSchedule::from_real_phaseflow(..).to_json_string()`
+/// (src/lie_svd_compiler.rs:59-88, :213-265); `events` as `MziPhase`
+/// (kind = the `PhaseRotorKind` variant's position).
+pub fn schedule_from_real_phaseflow_json(events: &[LsvdMziPhase], channels: usize, target: HardwareTarget) -> String {
+    text_call("lsvd_schedule_from_real_phaseflow", |buf, cap, len| unsafe {
+        lsvd_schedule_from_real_phaseflow(events.as_ptr(), events.len() as i64, channels as i64, target.code(), buf,
+            cap, len)
+    })
+}
+
+/// `HardwareSchedule::from_orthogonal_matrix(..).to_json_string()`
+/// (src/lie_svd_compiler.rs:144-198, :213-265).
+pub fn schedule_from_orthogonal_json(v: &Array2<f64>, target: HardwareTarget) -> String {
+    let d = v.nrows();
+    assert_eq!(d, v.ncols(), "HardwareSchedule::from_orthogonal_matrix: matrix must be square");
+    let a = contiguous(v);
+    text_call("lsvd_schedule_from_orthogonal", |buf, cap, len| unsafe {
+        lsvd_schedule_from_orthogonal(d as i64, a.as_ptr(), target.code(), buf, cap, len)
+    })
+}
+
+/// The binary phase-schedule frame of a rotor stream held on the host.
+pub fn schedule_binary_from_rotors(rotors: &[LsvdRotor], channels: usize, target: HardwareTarget) -> Vec<u8> {
+    let mut len = 0i64;
+    let st = unsafe {
+        lsvd_schedule_binary_from_rotors(std::ptr::null_mut(), rotors.as_ptr(), rotors.len() as i64, channels as i64,
+            target.code(), std::ptr::null_mut(), 0, &mut len, 0)
+    };
+    assert_eq!(st, LSVD_OK, "lsvd_schedule_binary_from_rotors sizing failed: {}", status_text(st));
+    let mut out = vec![0u8; len as usize];
+    let st = unsafe {
+        lsvd_schedule_binary_from_rotors(std::ptr::null_mut(), rotors.as_ptr(), rotors.len() as i64, channels as i64,
+            target.code(), out.as_mut_ptr() as *mut std::os::raw::c_void, len, &mut len, 0)
+    };
+    assert_eq!(st, LSVD_OK, "lsvd_schedule_binary_from_rotors failed: {}", status_text(st));
+    out
+}
+
+/// The phase-schedule-v1 JSON text of a binary frame.
+pub fn schedule_binary_to_json(frame: &[u8]) -> String {
+    text_call("lsvd_schedule_binary_to_json", |buf, cap, len| unsafe {
+        lsvd_schedule_binary_to_json(frame.as_ptr() as *const std::os::raw::c_void, frame.len() as i64, buf, cap, len)
+    })
+}
