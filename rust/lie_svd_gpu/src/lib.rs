@@ -10,6 +10,8 @@
 //! | `LieSvdMicro::solve` (src/lie_svd_micro.rs:21)               | [`micro_solve`]             |
 //! | `LieSvdJoint::diagonalize_symmetric_with_params` (src/lie_svd_joint.rs:71) | [`diagonalize_symmetric_with_params`] |
 //! | `LieSvdJoint::joint_svd_with_params` (src/lie_svd_joint.rs:170) | [`joint_svd_with_params`] |
+//! | `HardwareSchedule::from_real_phaseflow` + `to_json_string` (src/lie_svd_compiler.rs:59, :213) | [`schedule_from_real_phaseflow_json`] |
+//! | `HardwareSchedule::from_orthogonal_matrix` + `to_json_string` (src/lie_svd_compiler.rs:144, :213) | [`schedule_from_orthogonal_json`] |
 //!
 //! plus the batched and large entries that have no reference counterpart
 //! ([`svd_batched`], [`svd_large`]).  Errors panic with the library's
