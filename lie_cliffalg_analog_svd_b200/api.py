@@ -298,6 +298,30 @@ class LieSvdAdaptive:
     def choose_route(a, ctx: Context | None = None) -> str:
         return LieSvdAdaptive.analyze_matrix(a, ctx=ctx)["route"]
 
+    @staticmethod
+    def solve(a, ctx: Context | None = None):
+        """``LieSvdAdaptive::solve`` (src/lie_svd_adaptive.rs:83-85)."""
+        return LieSvdAdaptive.solve_with_trace(a, ctx=ctx)[0]
+
+    @staticmethod
+    def solve_with_trace(a, params=None, ctx: Context | None = None):
+        """``LieSvdAdaptive::solve_with_trace`` (src/lie_svd_adaptive.rs:87-100)
+        with the default ``LieSvdAdaptiveParams``: the triage picks the route
+        as the reference does; Micro and Small run as there, and the research
+        routes (PhaseFlow, CoreFlowTopo, Hybrid) run the exact Small tier
+        instead.  Returns ``((U, sigma, Vt), trace)``, trace = {"route": the
+        reference's route, "route_taken": the tier that ran, "triage": the
+        analyze_matrix statistics}."""
+        if params is not None:
+            raise L.LsvdError(L.UNSUPPORTED, "LieSvdAdaptive: only the default parameters are mirrored")
+        tri = LieSvdAdaptive.analyze_matrix(a, ctx=ctx)
+        route = tri["route"]
+        if route == "Micro":
+            res, taken = LieSvdMicro.solve(a, ctx=ctx), "Micro"
+        else:
+            res, taken = LieSvdSmall.solve(a, ctx=ctx), "Small"
+        return res, {"route": route, "route_taken": taken, "triage": tri}
+
 
 @dataclass
 class PhaseEngineReport:

@@ -62,6 +62,24 @@ def test_reference_routing_through_gpu():  # src/lie_svd_adaptive.rs:395-552
         LieSvdAdaptive.analyze_matrix(np.ones((3, 4)))
 
 
+def test_adaptive_solve_with_trace():  # src/lie_svd_adaptive.rs:83-100
+    # Small and Micro routes run as the reference runs them; a PhaseFlow route is
+    # reported and solved by the exact tier, to the same bars
+    for a, route, taken in ((np.diag(2.0 - np.arange(16) / 16), "Small", "Small"),
+                            (np.array([[3.0, 1.0], [0.5, 2.0]]), "Micro", "Micro"),
+                            (upper_shift(24, 1.0, 5.0), "PhaseFlow", "Small")):
+        (u, s, vt), tr = LieSvdAdaptive.solve_with_trace(a)
+        assert (tr["route"], tr["route_taken"]) == (route, taken)
+        assert tr["triage"]["route"] == route
+        so = (O.LieSvdMicro if a.shape[0] <= 4 else O.LieSvdSmall).solve(a)[1]
+        assert np.max(np.abs(s - so)) <= 1e-13 * so.max()
+        assert np.linalg.norm((u * s) @ vt - a) <= 4e-13 * np.linalg.norm(a)
+    u, s, vt = LieSvdAdaptive.solve(np.diag(2.0 - np.arange(16) / 16))
+    assert np.allclose(np.sort(s), np.sort(2.0 - np.arange(16) / 16), atol=1e-14)
+    with pytest.raises(L.LsvdError):
+        LieSvdAdaptive.solve_with_trace(np.eye(4), params={"small_max_n": 10})
+
+
 def test_batched_workload_routes():
     # the benchmark's uneven batch: every matrix gets its route on the device
     ns, a, _ = P.uneven_batch_workload(3000, seed=8)
