@@ -10,10 +10,10 @@ from .api import (Context, LieSvd, LieSvdMicro, LieSvdSmall, SmallResult, SvdMet
                   HardwareSchedule, JointDiagonalizationParams, LieSvdJoint, default_context,
                   PolarResult, SvdStream, metrics, packed_offsets, polar, svd_batched,
                   svd_batched_stream, svd_vjp, unpack, svd_large, LargeResult,
-                  LieSvdAdaptive, PhaseEngine, triage_batched)
+                  LieSvdAdaptive, PhaseEngine, triage_batched, solvers)
 from ._lib import LsvdError  # noqa: F401
 from .dist import svd_batched_sharded  # noqa: F401
 
 __all__ = ["Context", "HardwareSchedule", "JointDiagonalizationParams", "LieSvdJoint", "LieSvd", "LieSvdMicro", "LieSvdSmall", "SmallResult", "SvdMetrics",
            "PolarResult", "SvdStream", "svd_batched_stream", "svd_vjp", "default_context", "metrics", "packed_offsets", "polar", "svd_batched", "unpack", "LsvdError", "svd_large", "LargeResult",
-           "LieSvdAdaptive", "PhaseEngine", "triage_batched", "svd_batched_sharded"]
+           "LieSvdAdaptive", "PhaseEngine", "triage_batched", "svd_batched_sharded", "solvers"]

@@ -236,10 +236,11 @@ class LieSvdMicro:
 
 
 class LieSvd:
-    """The exact tiers of ``LieSvd::solve`` (src/lie_svd.rs:49): Micro for
-    n <= MICRO_MAX_N = 4, Small otherwise.  The adaptive triage that may send
-    structured inputs to the PhaseFlow/CoreFlow research routes is not part of
-    this library."""
+    """``LieSvd::solve`` (src/lie_svd.rs:49), which forwards to
+    ``LieSvdAdaptive::solve``: the tiers that runs here -- Micro for
+    n <= MICRO_MAX_N = 4, Small otherwise -- without computing the triage
+    (``LieSvdAdaptive.solve_with_trace`` reports the route the reference's
+    triage would pick, including its PhaseFlow/CoreFlow research routes)."""
 
     MICRO_MAX_N = 4
 
@@ -249,6 +250,25 @@ class LieSvd:
         if a.shape[0] <= LieSvd.MICRO_MAX_N:
             return LieSvdMicro.solve(a, ctx=ctx)
         return LieSvdSmall.solve(a, ctx=ctx)
+
+
+class solvers:  # noqa: N801 -- mirrors the Rust module name
+    """``solvers::run_small`` / ``run_auto`` (src/lib.rs:56-60, :117-121):
+    the SVD and its wall time in seconds (the reference returns a Duration)."""
+
+    @staticmethod
+    def run_small(a, ctx: Context | None = None):
+        import time
+        t0 = time.perf_counter()
+        u, s, vt = LieSvdSmall.solve(a, ctx=ctx)
+        return u, s, vt, time.perf_counter() - t0
+
+    @staticmethod
+    def run_auto(a, ctx: Context | None = None):
+        import time
+        t0 = time.perf_counter()
+        u, s, vt = LieSvd.solve(a, ctx=ctx)
+        return u, s, vt, time.perf_counter() - t0
 
 
 ADAPTIVE_ROUTES = ("Micro", "Small", "PhaseFlow", "CoreFlowTopo", "Hybrid")

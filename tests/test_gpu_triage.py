@@ -118,3 +118,12 @@ def test_phase_engine_facade():  # src/lie_svd_engine.rs:338-362
     v, diags, trace, rep = PhaseEngine.diagonalize_family(fam)
     assert rep.route == "JointPhaseJade" and rep.passport["family"] == 4 and rep.orth_v < 1e-10
     assert trace.final_offdiag < trace.initial_offdiag * 1e-8
+
+
+def test_solvers_mirror():  # src/lib.rs:56-60, :117-121
+    from lie_cliffalg_analog_svd_b200 import solvers
+    a = np.random.default_rng(8).standard_normal((20, 20))
+    so = O.LieSvdSmall.solve(a)[1]
+    for run in (solvers.run_small, solvers.run_auto):
+        u, s, vt, secs = run(a)
+        assert secs > 0 and np.max(np.abs(s - so)) <= 1e-13 * so.max()
