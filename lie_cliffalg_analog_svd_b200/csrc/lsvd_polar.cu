@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <vector>
 
@@ -236,10 +237,30 @@ cudaError_t launch_gemm_t(cudaStream_t st, const void* A, const void* B, float* 
     CUtensorMap ma, mb;
     if (!make_map(&ma, PREC, A, M, K, kTile) || !make_map(&mb, PREC, B, N, K, TN))
         return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<PREC, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         smem_bytes(TN));
+    // the persistent kernel (one CTA per SM, two TMEM accumulators, epilogue beside the next
+    // tile's main loop); LSVD_TC_GEMM_SIMPLE=1 selects the one-tile-per-CTA kernel
+    static const bool simple = [] {
+        const char* v = std::getenv("LSVD_TC_GEMM_SIMPLE");
+        return v && v[0] == '1';
+    }();
+    cudaError_t e;
+    if (simple) {
+        e = cudaFuncSetAttribute(tc_gemm_kernel<PREC, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem_bytes(TN));
+        if (e != cudaSuccess) return e;
+        tc_gemm_kernel<PREC, TN><<<dim3(N / TN, M / kTile), 128, smem_bytes(TN), st>>>(ma, mb, C, N, K, err);
+        return cudaGetLastError();
+    }
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    e = cudaFuncSetAttribute(tc_gemm_persistent_kernel<PREC, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem_bytes(TN));
     if (e != cudaSuccess) return e;
-    tc_gemm_kernel<PREC, TN><<<dim3(N / TN, M / kTile), 128, smem_bytes(TN), st>>>(ma, mb, C, N, K, err);
+    const int tiles = (M / kTile) * (N / TN);
+    tc_gemm_persistent_kernel<PREC, TN><<<std::max(1, std::min(tiles, sms)), 192, smem_bytes(TN), st>>>(
+        ma, mb, C, N, M, N, K, err);
     return cudaGetLastError();
 }
 

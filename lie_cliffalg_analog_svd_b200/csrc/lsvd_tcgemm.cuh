@@ -250,5 +250,176 @@ __global__ void __launch_bounds__(128, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
 }
 
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Persistent variant, grid = min(tiles, SMs), 192 threads (6 warps), one CTA
+// per SM, tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (row of tiles
+// major: consecutive CTAs share the A row panel in L2):
+//   warp 0 (one lane)  TMA producer over every (tile, K-slice) of the CTA;
+//   warp 1 (one lane)  MMA issuer; the accumulator of the CTA's i-th tile lives
+//                      in TMEM columns (i & 1) * TN .. + TN (2 TN allocated);
+//   warps 2..5         epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its
+//                      lane quadrant), stores FP32 rows, releases the accumulator.
+// So tile i's epilogue overlaps tile i + 1's main loop.  Barriers: full/empty
+// per stage, tfull[2] (MMA -> epilogue, tcgen05.commit), tempty[2] (epilogue ->
+// MMA, one arrival per epilogue warp).  Every wait is bounded; a timeout sets
+// an error code, the roles stop issuing, the producer drains its copies, the
+// MMA issuer waits (bounded) for its MMAs, and the CTA frees its TMEM.
+template <int PREC, int TN>
+__global__ void __launch_bounds__(192, 1)
+    tc_gemm_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                              float* __restrict__ C, int ldc, int M, int N, int K, int* err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages], tfull[2], tempty[2], mdone;
+    __shared__ uint32_t tmem_base;
+    __shared__ int s_err;
+    volatile int* verr = &s_err;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    constexpr int kStageBytes = stage_bytes(TN);
+    constexpr int elem = (PREC == kBF16) ? 2 : 4;
+    constexpr int kslice = kSliceBytes / elem;
+    constexpr int kmma = (PREC == kBF16) ? 16 : 8;
+    const int nk = K / kslice;
+    const int ntn = N / TN, tiles = (M / kTile) * ntn;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(smem_u32(&tfull[a]), 1);
+            mbar_init(smem_u32(&tempty[a]), 4);
+        }
+        mbar_init(smem_u32(&mdone), 1);
+        s_err = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base)),
+                     "r"(2 * TN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+
+    if (warp == 0 && lane == 0) {
+        int it = 0;  // K-slices issued (ring position)
+        bool stop = false;
+        for (int t = blockIdx.x; t < tiles && !stop; t += gridDim.x) {
+            const int m0 = (t / ntn) * kTile, n0 = (t % ntn) * TN;
+            for (int kb = 0; kb < nk; ++kb) {
+                const int s = it % kStages;
+                if (*verr || (it >= kStages && !mbar_wait(smem_u32(&empty[s]), ((it / kStages) - 1) & 1))) {
+                    if (!*verr) *verr = 1;
+                    stop = true;
+                    break;
+                }
+                const uint32_t a_dst = base + s * kStageBytes;
+                const uint32_t b_dst = a_dst + kTile * kSliceBytes;
+                mbar_expect_tx(smem_u32(&full[s]), kStageBytes);
+                tma_load_2d(a_dst, &mapA, smem_u32(&full[s]), kb * kslice, m0);
+                tma_load_2d(b_dst, &mapB, smem_u32(&full[s]), kb * kslice, n0);
+                ++it;
+            }
+        }
+        // drain: every copy issued lands before the CTA leaves
+        if (stop)
+            for (int j = (it > kStages ? it - kStages : 0); j < it; ++j)
+                mbar_wait(smem_u32(&full[j % kStages]), (j / kStages) & 1);
+    } else if (warp == 1 && lane == 0) {
+        int it = 0, lt = 0;
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++lt) {
+            const int acc = lt & 1;
+            if (*verr || (lt >= 2 && !mbar_wait(smem_u32(&tempty[acc]), ((lt >> 1) - 1) & 1))) {
+                if (!*verr) *verr = 2;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t d = tmem + uint32_t(acc * TN);
+            bool stop = false;
+            for (int kb = 0; kb < nk; ++kb, ++it) {
+                const int s = it % kStages;
+                if (!mbar_wait(smem_u32(&full[s]), (it / kStages) & 1)) {
+                    *verr = 3;
+                    stop = true;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t a_src = base + s * kStageBytes;
+                const uint32_t b_src = a_src + kTile * kSliceBytes;
+                const uint64_t da = smem_desc(a_src), db = smem_desc(b_src);
+#pragma unroll
+                for (int k = 0; k < kslice / kmma; ++k) {
+                    const uint64_t off = uint64_t((k * kmma * elem) >> 4);
+                    mma<PREC, TN>(d, da + off, db + off, (kb > 0 || k > 0) ? 1u : 0u);
+                }
+                mma_commit(smem_u32(&empty[s]));
+            }
+            if (stop) break;
+            mma_commit(smem_u32(&tfull[acc]));
+        }
+        // every MMA this thread issued is complete before TMEM can be freed
+        mma_commit(smem_u32(&mdone));
+        if (!mbar_wait(smem_u32(&mdone), 0) && !*verr) *verr = 5;
+    } else if (warp >= 2) {
+        const int q = warp & 3;  // the TMEM lane quadrant this warp may read
+        int lt = 0;
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++lt) {
+            const int acc = lt & 1;
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&tfull[acc]), (lt >> 1) & 1));
+            if (!ok || *verr) {
+                if (!ok && lane == 0) *verr = 4;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const int m0 = (t / ntn) * kTile, n0 = (t % ntn) * TN;
+            float* crow = C + size_t(m0 + q * 32 + lane) * ldc + n0;
+#pragma unroll 1
+            for (int c0 = 0; c0 < TN; c0 += 32) {
+                uint32_t v[32];
+                const uint32_t taddr = tmem + (uint32_t(q * 32) << 16) + uint32_t(acc * TN + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                    "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                      "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                      "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+                      "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                      "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                      "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 32; j += 4) {
+                    float4 f;
+                    f.x = __uint_as_float(v[j]);
+                    f.y = __uint_as_float(v[j + 1]);
+                    f.z = __uint_as_float(v[j + 2]);
+                    f.w = __uint_as_float(v[j + 3]);
+                    *reinterpret_cast<float4*>(crow + c0 + j) = f;
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&tempty[acc]));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (threadIdx.x == 0 && *verr) atomicExch(err, *verr);
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TN));
+}
+
 }  // namespace tc
 }  // namespace lsvd
