@@ -10,8 +10,8 @@
 // One CTA of 8 warps computes a 128 x 128 tile (or 128 x 64 when the product
 // has too few 128 x 128 tiles to fill the GPU twice); warps are arranged 4 (M)
 // x 2 (N) and own 32 x 64 (32 x 32) each (4 x 8 (4 x 4) tiles of 8 x 8).
-// Operands stream through a 4-stage cp.async ring of BK = 16; each operand
-// tile sits in shared memory either K-contiguous (leading dimension 20
+// Operands stream through a 3-stage cp.async ring of BK = 32; each operand
+// tile sits in shared memory either K-contiguous (leading dimension 36
 // doubles) or M/N-contiguous (leading dimension 132 doubles), both = 4 mod 16,
 // so the 8 x 4 fragment reads of a half-warp hit 16 distinct 8-byte bank
 // pairs.  Edges are zero-filled by the cp.async source size; the caller keeps
@@ -25,11 +25,11 @@
 namespace lsvd {
 namespace dg {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4, THREADS = 256;
-constexpr int LDK = BK + 4;   // K-contiguous tiles: [128][20]
-constexpr int LDMN = BM + 4;  // M/N-contiguous tiles: [16][132]
-constexpr int TILE_DOUBLES = (BM * LDK > BK * LDMN) ? BM * LDK : BK * LDMN;  // 2560
-constexpr int SMEM_BYTES = STAGES * 2 * TILE_DOUBLES * 8;                       // 163840
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 256;
+constexpr int LDK = BK + 4;   // K-contiguous tiles: [128][36]
+constexpr int LDMN = BM + 4;  // M/N-contiguous tiles: [32][132]
+constexpr int TILE_DOUBLES = (BM * LDK > BK * LDMN) ? BM * LDK : BK * LDMN;  // 4608
+constexpr int SMEM_BYTES = STAGES * 2 * TILE_DOUBLES * 8;                       // 221184
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -55,12 +55,13 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 template <bool KCONT, int R = 128>
 __device__ __forceinline__ void load_tile(double* sm, const double* X, int64_t ldx, int r0, int rdim,
                                           int k0, int kdim, int tid) {
+    constexpr int KCH = BK / 2;  // two-double chunks per row of a slice
     if (KCONT) {
-        // R rows x 16 k = 8 R chunks of two doubles
+        // R rows x BK k = KCH R chunks of two doubles
 #pragma unroll
-        for (int it = 0; it < R / 32; ++it) {
+        for (int it = 0; it < R * KCH / THREADS; ++it) {
             const int c = tid + it * THREADS;
-            const int row = c >> 3, kc = (c & 7) * 2;
+            const int row = c / KCH, kc = (c % KCH) * 2;
             const int gr = r0 + row, gk = k0 + kc;
             int valid = kdim - gk;
             valid = valid > 2 ? 2 : (valid < 0 ? 0 : valid);
@@ -69,9 +70,9 @@ __device__ __forceinline__ void load_tile(double* sm, const double* X, int64_t l
             cp_async16(sm + row * LDK + kc, src, valid * 8);
         }
     } else {
-        // 16 k-rows x R = 8 R chunks
+        // BK k-rows x R = KCH R chunks
 #pragma unroll
-        for (int it = 0; it < R / 32; ++it) {
+        for (int it = 0; it < R * KCH / THREADS; ++it) {
             const int c = tid + it * THREADS;
             const int kr = c / (R / 2), mc = (c % (R / 2)) * 2;
             const int gk = k0 + kr, gm = r0 + mc;
