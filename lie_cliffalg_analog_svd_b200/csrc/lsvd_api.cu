@@ -289,6 +289,7 @@ extern "C" lsvd_status lsvd_small_solve_f64(lsvd_context* ctx, int64_t n, const 
                                             double* Vt, int64_t ldvt, lsvd_diag* diag,
                                             lsvd_rotor* rotors, int64_t rotor_cap,
                                             int64_t* rotor_count, int32_t* perm, uint32_t flags) {
+    LSVD_TRACE("lsvd_small_solve_f64");
     if (ctx && n > kMaxN) {
         // beyond the shared-memory kernels: the blocked large solve (no plane-rotation stream)
         if (rotors || rotor_count || perm)
@@ -318,6 +319,7 @@ extern "C" lsvd_status lsvd_micro_solve_f64(lsvd_context* ctx, int64_t n, const 
                                             int64_t lda, double* U, int64_t ldu, double* S,
                                             double* Vt, int64_t ldvt, lsvd_diag* diag,
                                             uint32_t flags) {
+    LSVD_TRACE("lsvd_micro_solve_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (n < 0 || n > 4) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "LieSvdMicro only supports N <= 4");
     if (n == 0) return LSVD_OK;  // empty result, src/lie_svd_micro.rs:27-31
@@ -543,6 +545,7 @@ static cudaError_t enqueue_plan(lsvd_context* ctx, BatchPlan& P, const double* A
 
 lsvd_status lsvd_run_plan(lsvd_context* ctx, BatchPlan& P, const double* A, double* U, double* S,
                           double* Vt, lsvd_diag* diag, bool want_diag, bool use_graph) {
+    LSVD_TRACE("batched/run_plan");
     const int sm_bytes = std::max(P.smem_bytes, 16);
     cudaError_t e = P.precision == LSVD_PREC_MIXED_TF32
                         ? cudaFuncSetAttribute(batched_mixed_kernel<kPrecTF32>,
@@ -591,6 +594,7 @@ static bool plan_matches(const BatchPlan& P, int64_t count, const int32_t* n, ls
 
 BatchPlan* lsvd_get_plan(lsvd_context* ctx, int64_t count, const int32_t* n, lsvd_precision prec,
                          lsvd_status* st) {
+    LSVD_TRACE("batched/plan");
     const uint64_t key = hash_ns(count, n) ^ (uint64_t(prec) << 61);
     auto it = ctx->plans.find(key);
     if (it != ctx->plans.end() && plan_matches(*it->second, count, n, prec)) {
@@ -651,6 +655,7 @@ static void lcg_gauss(uint64_t& st, double* out, size_t count) {
 
 extern "C" lsvd_status lsvd_autotune_f64(lsvd_context* ctx, int64_t per_class, const char* cache_path,
                                          char* report, int64_t report_cap) {
+    LSVD_TRACE("lsvd_autotune_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (per_class < 16 || per_class > 100000)
         return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_autotune_f64: per_class in 16..100000");
@@ -802,6 +807,7 @@ constexpr int kPipeWeight[kPipeChunks] = {1, 2, 3, 4, 4, 3, 2, 1};
 static lsvd_status batched_pipelined(lsvd_context* ctx, int64_t count, const int32_t* n, const double* A,
                                      double* U, double* S, double* Vt, lsvd_diag* diags,
                                      lsvd_precision precision, bool want_diag) {
+    LSVD_TRACE("batched/host_pipeline");
     constexpr int C = kPipeChunks;
     cudaError_t e = cudaSuccess;
     if (!ctx->h2d_stream && (e = cudaStreamCreateWithFlags(&ctx->h2d_stream, cudaStreamNonBlocking)) != cudaSuccess)
@@ -923,6 +929,7 @@ extern "C" lsvd_status lsvd_svd_batched_f64(lsvd_context* ctx, int64_t count, co
                                             const double* A, double* U, double* S, double* Vt,
                                             lsvd_diag* diags, lsvd_precision precision,
                                             uint32_t flags) {
+    LSVD_TRACE("lsvd_svd_batched_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (count < 0 || (count > 0 && (!n || !A || !U || !S || !Vt)))
         return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_svd_batched_f64: bad pointer");

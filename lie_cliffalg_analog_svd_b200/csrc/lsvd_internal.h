@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "lsvd.h"
+#include "lsvd_trace.h"
 
 namespace lsvd {
 constexpr int kMaxClasses = 8;

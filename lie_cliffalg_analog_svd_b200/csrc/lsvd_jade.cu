@@ -515,6 +515,7 @@ extern "C" lsvd_status lsvd_jade_sym_f64(lsvd_context* ctx, int64_t families, in
                                          const double* M, const lsvd_joint_params* params,
                                          double* V, double* diag, lsvd_joint_trace* traces,
                                          uint32_t flags) {
+    LSVD_TRACE("lsvd_jade_sym_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (families < 0 || K < 0 || n < 0) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "LieSvdJoint: bad shape");
     if (families == 0) return LSVD_OK;

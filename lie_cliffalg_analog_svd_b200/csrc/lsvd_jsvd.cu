@@ -490,6 +490,7 @@ extern "C" lsvd_status lsvd_joint_svd_f64(lsvd_context* ctx, int64_t families, i
                                           int64_t cols, const double* M, const lsvd_joint_params* params,
                                           double* U, double* sig, double* Vt, lsvd_joint_trace* traces,
                                           uint32_t flags) {
+    LSVD_TRACE("lsvd_joint_svd_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (families < 0 || K < 0 || rows < 0 || cols < 0)
         return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "LieSvdJoint::joint_svd: bad shape");

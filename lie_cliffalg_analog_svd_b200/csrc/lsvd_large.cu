@@ -950,6 +950,7 @@ static lsvd_status run_sweeps(lsvd_context* ctx, double* H, int64_t ldh, int gm,
                               double tol_conv, double scale2, int max_sweeps, int inner_max, char* ws,
                               int* sweeps_out, int64_t* rot_out, double* off_out, int* inner_cap_out,
                               double* ms_out) {
+    LSVD_TRACE("large/jacobi_one_sided");
     cudaStream_t st = ctx->stream;
     const int nb = npad / BW;
     const int npairs = nb / 2;
@@ -1111,6 +1112,7 @@ static void twoside_tiles(int nb, std::vector<int>& tiles, std::vector<int>& n1)
 static lsvd_status run_sweeps2(lsvd_context* ctx, double* P, double* Vc, int n, int npad, double limit, double tau,
                                int max_sweeps, int inner_max, char* ws, int* sweeps_out, int64_t* rot_out,
                                double* off_out, int* inner_cap_out, double* ms_out) {
+    LSVD_TRACE("large/jacobi_two_sided");
     cudaStream_t st = ctx->stream;
     const int nb = npad / BW;
     const int npairs = nb / 2;
@@ -1347,6 +1349,7 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
         // TF32/BF16 tensor-core bulk only (no FP64 iterations): its factor Q0
         // preconditions the eigensolve below and accuracy comes from the FP64
         // cleanup on A itself.
+        LSVD_TRACE("large/polar");
         pst = lsvd_polar_run(ctx, m, n, A64, ld, lowp ? precision : LSVD_PREC_FP64, lowp ? 0 : 120, &X, &ldx,
                              &pinfo);
         if (pst != LSVD_OK && pst != LSVD_NOT_CONVERGED) return pst;
@@ -1531,6 +1534,7 @@ static lsvd_status large_impl(lsvd_context* ctx, int64_t m, int64_t n, const dou
     ctx->launches += 3;
     total.stop(st);
     // 5. outputs: the thin SVD of A, or of A^T for a transposed input (U and Vt swap roles)
+    LSVD_TRACE("large/outputs");
     double* dS = sig;  // sorted sigma back to the device for the diagnostics
     if ((e = cudaMemcpyAsync(dS, hsorted.data(), size_t(n) * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return lsvd_ctx_cuda(ctx, e, "large: sorted sigma");
@@ -1632,6 +1636,7 @@ lsvd_status lsvd_large_solve(lsvd_context* ctx, int64_t rows, int64_t cols, cons
 extern "C" lsvd_status lsvd_svd_large_f64(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,
                                           double* U, int64_t ldu, double* S, double* Vt, int64_t ldvt,
                                           lsvd_precision precision, lsvd_large_info* info, uint32_t flags) {
+    LSVD_TRACE("lsvd_svd_large_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (m < 1 || n < 1) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "lsvd_svd_large_f64: empty matrix");
     const int64_t k = std::min(m, n);

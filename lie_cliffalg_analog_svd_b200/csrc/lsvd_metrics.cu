@@ -125,6 +125,7 @@ extern "C" lsvd_status lsvd_metrics_f64(lsvd_context* ctx, int64_t m, int64_t d,
                                         const double* A, const double* U, const double* S,
                                         const double* Vt, const double* sigma_ref, double* out,
                                         uint32_t flags) {
+    LSVD_TRACE("lsvd_metrics_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (m <= 0 || d <= 0 || k <= 0 || k > (m < d ? m : d))
         return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "lsvd_metrics_f64: bad shape");

@@ -344,6 +344,7 @@ int noalloc_smem_bytes(const ClassCfg* cls) {
 extern "C" lsvd_status lsvd_svd_batched_noalloc_f64(void* stream, int64_t count, const int32_t* n,
                                                     const double* A, double* U, double* S,
                                                     double* Vt, lsvd_diag* diags, uint32_t flags) {
+    LSVD_TRACE("lsvd_svd_batched_noalloc_f64");
     if (count < 0 || (count > 0 && (!n || !A || !U || !S || !Vt))) return LSVD_BAD_ARGUMENT;
     if (count > kMaxCount) return LSVD_UNSUPPORTED;  // more matrices than the scratch holds
     if (count == 0) return LSVD_OK;

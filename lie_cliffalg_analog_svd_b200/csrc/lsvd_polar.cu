@@ -302,6 +302,7 @@ struct GemmTimer {
 extern "C" lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N, int64_t K,
                                          const float* A, const float* B, float* C,
                                          lsvd_precision precision) {
+    LSVD_TRACE("lsvd_gemm_nt_lowp");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (precision != LSVD_PREC_MIXED_TF32 && precision != LSVD_PREC_MIXED_BF16)
         return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_gemm_nt_lowp: precision must be TF32 or BF16");
@@ -344,6 +345,7 @@ extern "C" lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N
 extern "C" lsvd_status lsvd_gemm_f64(lsvd_context* ctx, int32_t trans_a, int32_t trans_b, int64_t M,
                                      int64_t N, int64_t K, double alpha, const double* A, int64_t lda,
                                      const double* B, int64_t ldb, double beta, double* C, int64_t ldc) {
+    LSVD_TRACE("lsvd_gemm_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (M < 0 || N < 0 || K < 0 || M > (1 << 24) || N > (1 << 24) || K > (1 << 24))
         return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "lsvd_gemm_f64: bad sizes");
@@ -361,6 +363,7 @@ extern "C" lsvd_status lsvd_gemm_f64(lsvd_context* ctx, int32_t trans_a, int32_t
 lsvd_status lsvd_polar_run(lsvd_context* ctx, int64_t m, int64_t n, const double* A, int64_t lda,
                            lsvd_precision precision, int fp64_cap, double** Xout, int64_t* ldx_out,
                            lsvd_polar_info* info) {
+    LSVD_TRACE("polar/newton_schulz");
     const bool lowp = precision == LSVD_PREC_MIXED_TF32 || precision == LSVD_PREC_MIXED_BF16;
     if (lowp && (m % kTile || n % kTile))
         return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "polar: TF32/BF16 need m, n multiples of 128");
@@ -530,6 +533,7 @@ lsvd_status lsvd_polar_run(lsvd_context* ctx, int64_t m, int64_t n, const double
 extern "C" lsvd_status lsvd_polar_f64(lsvd_context* ctx, int64_t m, int64_t n, const double* A,
                                       int64_t lda, double* Q, int64_t ldq, lsvd_precision precision,
                                       lsvd_polar_info* info, uint32_t flags) {
+    LSVD_TRACE("lsvd_polar_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (m <= 0 || n <= 0 || m < n) return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "polar: need m >= n >= 1");
     if (!A || !Q || lda < n || ldq < n) return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "polar: bad pointer");

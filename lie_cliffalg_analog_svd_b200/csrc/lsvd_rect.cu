@@ -88,6 +88,7 @@ extern "C" lsvd_status lsvd_small_solve_rectangular_f64(lsvd_context* ctx, int64
                                                         int64_t ldu, double* S, double* Vt,
                                                         int64_t ldvt, lsvd_diag* diag,
                                                         uint32_t flags) {
+    LSVD_TRACE("lsvd_small_solve_rectangular_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (m <= 0 || d <= 0)
         return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "LieSvdSmall::solve_rectangular: empty input");

@@ -61,6 +61,7 @@ extern "C" LSVD_API lsvd_status lsvd_schedule_binary_from_rotors(lsvd_context* c
                                                                  int64_t count, int64_t channels, int32_t target,
                                                                  void* out, int64_t cap, int64_t* len,
                                                                  uint32_t flags) {
+    LSVD_TRACE("lsvd_schedule_binary_from_rotors");
     if (count < 0 || channels < 0 || (count > 0 && !rotors) || (target != 0 && target != 1) ||
         (flags & ~(LSVD_DEVICE_POINTERS | LSVD_ASYNC)) != 0)
         return LSVD_BAD_ARGUMENT;

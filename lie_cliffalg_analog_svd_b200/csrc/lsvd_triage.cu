@@ -354,6 +354,7 @@ __global__ void __launch_bounds__(TT) triage_kernel(const TriageArgs args) {
 extern "C" lsvd_status lsvd_triage_batched_f64(lsvd_context* ctx, int64_t count, const int32_t* rows,
                                                const int32_t* cols, const double* A, lsvd_triage* out,
                                                uint32_t flags) {
+    LSVD_TRACE("lsvd_triage_batched_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (count < 0 || (count > 0 && (!rows || !cols || !A || !out)))
         return lsvd_ctx_fail(ctx, LSVD_BAD_ARGUMENT, "lsvd_triage_batched_f64: bad pointer");

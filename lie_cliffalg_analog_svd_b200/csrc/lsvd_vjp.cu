@@ -488,6 +488,7 @@ extern "C" lsvd_status lsvd_svd_batched_stream_f64(lsvd_context* ctx, int64_t co
                                                    lsvd_rotor* rotors, int64_t rotor_cap,
                                                    int64_t* rotor_count, int32_t* perm, lsvd_diag* diags,
                                                    uint32_t flags) {
+    LSVD_TRACE("lsvd_svd_batched_stream_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (count < 0 || m < 1 || n < 1 || m < n)
         return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "svd_batched_stream: need m >= n >= 1");
@@ -610,6 +611,7 @@ extern "C" lsvd_status lsvd_svd_vjp_f64(lsvd_context* ctx, int64_t count, int64_
                                         const int64_t* rotor_count, const double* Ubar,
                                         const double* Sbar, const double* Vbar, const double* Qbar,
                                         const double* Vt, double gap_tol, double* Abar, uint32_t flags) {
+    LSVD_TRACE("lsvd_svd_vjp_f64");
     if (!ctx) return LSVD_BAD_ARGUMENT;
     if (count < 0 || m < 1 || n < 1 || m < n)
         return lsvd_ctx_fail(ctx, LSVD_BAD_SHAPE, "svd_vjp: need m >= n >= 1");
