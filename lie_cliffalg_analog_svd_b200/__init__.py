@@ -13,7 +13,11 @@ from .api import (Context, LieSvd, LieSvdMicro, LieSvdSmall, SmallResult, SvdMet
                   LieSvdAdaptive, PhaseEngine, triage_batched, solvers)
 from ._lib import LsvdError  # noqa: F401
 from .dist import svd_batched_sharded  # noqa: F401
+from .consumers import (CanonicalOrder, LieSvdBss, PhaseBssParams,  # noqa: F401
+                        diagonalize_symmetric_canonicalized, solve_canonicalized)
 
 __all__ = ["Context", "HardwareSchedule", "JointDiagonalizationParams", "LieSvdJoint", "LieSvd", "LieSvdMicro", "LieSvdSmall", "SmallResult", "SvdMetrics",
            "PolarResult", "SvdStream", "svd_batched_stream", "svd_vjp", "default_context", "metrics", "packed_offsets", "polar", "svd_batched", "unpack", "LsvdError", "svd_large", "LargeResult",
-           "LieSvdAdaptive", "PhaseEngine", "triage_batched", "svd_batched_sharded", "solvers"]
+           "LieSvdAdaptive", "PhaseEngine", "triage_batched", "svd_batched_sharded", "solvers",
+           "LieSvdBss", "PhaseBssParams", "CanonicalOrder", "solve_canonicalized",
+           "diagonalize_symmetric_canonicalized"]
