@@ -21,7 +21,10 @@ Other workloads (each prints its own JSON line):
   single : one 64x64 Gaussian through the exact polar/Jacobi route (SVDs/s);
   adjoint: SVD/polar vector-Jacobian products of 4,096 matrices 128x64 (sigma
            uniform in [0.1, 10], gap >= 1e-3, 10% with one 1e-6 gap) from the
-           stored rotor streams, cotangents N(0,1) on U, S, V and U V^T (VJPs/s).
+           stored rotor streams, cotangents N(0,1) on U, S, V and U V^T (VJPs/s);
+  bss    : Phase-BSS (LieSvdBss.separate) of 32 mixed sinusoid-plus-noise
+           channels x 2^20 samples from host arrays, lags {1, 2, 3, 5}
+           (samples/s, copies inside the step).
 
 Prints ONE JSON line (rank 0).  ``value`` is SVDs/s of the whole job with the
 inputs resident in HBM (CUDA events on the launching stream, max over ranks);
@@ -71,7 +74,7 @@ def parse():
                     help="batched workload on N GPUs: weak = a full batch per rank; strong = one "
                          "batch split into cost-balanced contiguous shards")
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "polar", "jade", "single", "adjoint", "svd_large"])
+                    choices=["batched", "polar", "jade", "single", "adjoint", "svd_large", "bss"])
     ap.add_argument("--families", type=int, default=512)
     ap.add_argument("--polar-size", default="full", choices=["full", "small"],
                     help="small: 2048x2048 and 4096x1024 instead of 4096x4096 and 8192x2048")
@@ -1057,6 +1060,95 @@ def run_reference_single(args):
     return 0
 
 
+BSS_CHANNELS, BSS_SAMPLES, BSS_LAGS = 32, 1 << 20, [1, 2, 3, 5]
+
+
+def bss_flops(ch, s, lags):
+    """FP64 flops of the products of one separation: channel means and the
+    centring update (inner dimension 2), covariance, whitening, one lagged
+    covariance per lag, separation."""
+    return 8.0 * ch * s + 2.0 * ch * ch * (3 * s + sum(s - g for g in lags if 0 < g < s))
+
+
+def run_bss(args):
+    torch, ws, rank, local, device = _init_dist()
+    from lie_cliffalg_analog_svd_b200 import Context, LieSvdBss, PhaseBssParams
+    from lie_cliffalg_analog_svd_b200 import profiles as P
+    from lie_cliffalg_analog_svd_b200.consumers import estimate_sir_db
+    ctx = Context(local)
+    ch, s = BSS_CHANNELS, BSS_SAMPLES
+    src, _, obs = P.bss_workload(ch, s, args.seed + rank)
+    params = PhaseBssParams.for_channels(ch)
+    params.lags = list(BSS_LAGS)
+    r = LieSvdBss.separate(obs, params, ctx=ctx)  # validation (untimed)
+    sir_before, sir_after = estimate_sir_db(src, obs), estimate_sir_db(src, r.separated)
+    for _ in range(args.warmup):
+        LieSvdBss.separate(obs, params, ctx=ctx)
+    torch.cuda.synchronize()
+    l0 = ctx.kernel_launches
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            LieSvdBss.separate(obs, params, ctx=ctx)
+        torch.cuda.synchronize()
+        el = _max_over_ranks(torch, ws, device, (time.perf_counter() - t0) / args.steps)
+    launches = (ctx.kernel_launches - l0) // max(args.steps, 1)
+    h2d, d2h = obs.nbytes, obs.nbytes + ch * ch * 8 * (len(BSS_LAGS) + 2)
+    line = _base_line(args, "samples/s", ws * s / el, el * 1e3, ws, f"phase_bss_{ch}ch_{s}samples",
+                      {"channels": ch, "samples": s, "lags": BSS_LAGS,
+                       "l2": f"observations {obs.nbytes / 1e6:.0f} MB per step, larger than the 126 MB L2"}, "f64")
+    fl = bss_flops(ch, s, BSS_LAGS)
+    line.update({
+        "e2e": {"value": ws * s / el, "unit": "samples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": el * 1e3},
+        "note": "value = e2e: LieSvdBss.separate takes host arrays (the reference's API), so the copies are "
+                "inside every step; the products are 2C^2T-sized GEMMs on the FP64 product kernel",
+        "products_gflop_per_step": fl / 1e9,
+        "copy_gbs": (h2d + d2h) / el / 1e9,
+        "accuracy": {"sir_db_before": sir_before, "sir_db_after": sir_after,
+                     "joint_initial_offdiag": r.trace.joint_initial_offdiag,
+                     "joint_final_offdiag": r.trace.joint_final_offdiag},
+        "gpu_launches": int(launches), "clocks": clk.summary()})
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = _bss_cpu_sample(args)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def _bss_cpu_sample(args, samples=1 << 17):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_consumers as OC  # noqa: E402
+    from lie_cliffalg_analog_svd_b200 import profiles as P
+    _, _, obs = P.bss_workload(BSS_CHANNELS, samples, args.seed)
+    p = OC.PhaseBssParams.for_channels(BSS_CHANNELS)
+    p.lags = list(BSS_LAGS)
+    t0 = time.perf_counter()
+    OC.bss_separate(obs, p)
+    el = time.perf_counter() - t0
+    return {"value": samples / el, "unit": "samples/s", "cores": 1, "kind": "port",
+            "sample": f"one separation of {BSS_CHANNELS} channels x {samples} samples of the same generator, "
+                      f"{el:.2f} s (oracle/oracle_consumers.py: the reference's per-sample lagged-covariance "
+                      "loop, products in ndarray order)"}
+
+
+def run_reference_bss(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    cb = _bss_cpu_sample(args)
+    el = BSS_SAMPLES / cb["value"]
+    line = _base_line(args, "samples/s", cb["value"], el * 1e3, args.gpus,
+                      f"phase_bss_{BSS_CHANNELS}ch_{BSS_SAMPLES}samples (reference CPU, bounded sample)",
+                      {"channels": BSS_CHANNELS, "samples": BSS_SAMPLES, "lags": BSS_LAGS, "l2": "n/a (CPU)"},
+                      "f64")
+    line.update({"impl": "reference", "cpu_baseline": cb,
+                 "e2e": {"value": cb["value"], "unit": "samples/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 ADJ_COUNT, ADJ_M, ADJ_N = 4096, 128, 64
 
 
@@ -1251,9 +1343,11 @@ def main():
     if args.impl == "reference":
         return {"batched": run_reference, "polar": run_reference_polar,
                 "jade": run_reference_jade, "single": run_reference_single,
-                "adjoint": run_reference_adjoint, "svd_large": run_reference_svd_large}[args.workload](args)
+                "adjoint": run_reference_adjoint, "svd_large": run_reference_svd_large,
+                "bss": run_reference_bss}[args.workload](args)
     return {"batched": run_b200, "polar": run_polar, "jade": run_jade,
-            "single": run_single, "adjoint": run_adjoint, "svd_large": run_svd_large}[args.workload](args)
+            "single": run_single, "adjoint": run_adjoint, "svd_large": run_svd_large,
+            "bss": run_bss}[args.workload](args)
 
 
 if __name__ == "__main__":

@@ -3,14 +3,15 @@ src/lie_svd_bss.rs) and the phase normalizer's canonical-order wrappers
 (src/phase_normalizer.rs:103-340).
 
 Device work: every product -- channel means, covariance, whitening, lagged
-covariances, separation, unmixing, row Gram matrices -- runs on the
-library's FP64 product kernel (``lsvd_gemm_f64``), and every solve on
-``LieSvdSmall`` (covariance SVD), ``LieSvdSmall.solve_rectangular``
-(leverage scores, the canonical solve) or Phase-JADE.  Host work is
-channels x channels glue: the whitening matrix from the covariance's SVD,
-symmetrising the lagged covariances, the wedge capacities of a Gram matrix,
-the permutation bookkeeping, and the reference's evaluation helpers
-(``channel_phase_coherence``, ``estimate_sir_db``) on returned arrays."""
+covariances, separation, unmixing, the coherence sums, row Gram matrices --
+runs on the library's FP64 product kernel (``lsvd_gemm_f64``, which splits
+a long inner dimension across the SMs), and every solve on ``LieSvdSmall``
+(covariance SVD), ``LieSvdSmall.solve_rectangular`` (leverage scores, the
+canonical solve) or Phase-JADE.  Host work is channels x channels glue: the
+whitening matrix from the covariance's SVD, symmetrising the lagged
+covariances, the wedge capacities of a Gram matrix, the permutation
+bookkeeping.  The reference's evaluation helpers (``channel_phase_coherence``,
+``estimate_sir_db``) are also provided for host arrays."""
 from __future__ import annotations
 
 from dataclasses import dataclass, field
@@ -93,6 +94,25 @@ def channel_phase_coherence(channels) -> np.ndarray:
     return np.clip(0.5 * lock + 0.5 * smooth, 0.0, 1.0)
 
 
+def _coherence_on_device(S, ctx: Context) -> np.ndarray:
+    """``channel_phase_coherence`` of the device rows ``S`` (channels x T,
+    T >= 2) from two products on the device: sum x_t^2 = diag(S S^T) and the
+    circular lag-1 sum x_t x_(t+1 mod T) = diag(S_(+1) S^T) plus the wrap-around
+    term; the gradient norm is 2 (sum x^2 - sum x x_(+1)) since the circular
+    shift keeps sum y^2 = sum x^2."""
+    ch, s = S.shape
+    g0 = _host(gemm_f64(S, S, trans_b=True, c=_even(ch, ch, S.device), ctx=ctx))
+    ahead = _even(ch, s - 1, S.device)
+    ahead.copy_(S[:, 1:])
+    g1 = _host(gemm_f64(ahead, S[:, :s - 1], trans_b=True, c=_even(ch, ch, S.device), ctx=ctx))
+    ends = _host(S[:, [0, s - 1]])
+    norm = np.diag(g0).copy()
+    delay = np.diag(g1) + ends[:, 0] * ends[:, 1]
+    n = np.maximum(norm, 1e-300)
+    grad = np.maximum(2.0 * (norm - delay), 0.0)
+    return np.clip(0.5 * np.abs(delay) / n + 0.5 / (1.0 + np.sqrt(grad / n)), 0.0, 1.0)
+
+
 def estimate_sir_db(reference, separated) -> float:
     """src/lie_svd_bss.rs:129-159: greedy matching on the absolute
     correlation matrix; signal-to-interference ratio in dB."""
@@ -155,9 +175,10 @@ class LieSvdBss:
             lagged.append(_host(gemm_f64(Wh, Wh, trans_b=True, alpha=1.0 / s, c=_even(ch, ch, dev), ctx=ctx)))
         basis, _, tr = LieSvdJoint.diagonalize_symmetric_with_params(lagged, params.joint, ctx=ctx)
         V = _to_dev(basis, dev)
-        sep = _host(gemm_f64(V, Wh, trans_a=True, c=_even(ch, s, dev), ctx=ctx))
+        Sep = gemm_f64(V, Wh, trans_a=True, c=_even(ch, s, dev), ctx=ctx)
         unmix = _host(gemm_f64(V, W, trans_a=True, c=_even(ch, ch, dev), ctx=ctx))
-        coh = channel_phase_coherence(sep)
+        coh = _coherence_on_device(Sep, ctx)
+        sep = _host(Sep)
         return PhaseBssResult(unmix, sep, coh,
                               PhaseBssTrace(ch, s, floor, tr.initial_offdiag, tr.final_offdiag, tr.rotations,
                                             float(coh.sum() / max(len(coh), 1))))

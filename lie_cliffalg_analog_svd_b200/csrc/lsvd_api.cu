@@ -115,7 +115,7 @@ lsvd_context::~lsvd_context() {
     cudaSetDevice(device);
     for (auto& kv : plans) kv.second.reset();
     for (auto& pp : pipe_plans) pp.reset();
-    for (auto* b : {&ws_a, &ws_u, &ws_s, &ws_vt, &ws_diag, &ws_misc, &ws_rot, &ws_polar, &ws_large})
+    for (auto* b : {&ws_a, &ws_u, &ws_s, &ws_vt, &ws_diag, &ws_misc, &ws_rot, &ws_polar, &ws_large, &ws_splitk})
         b->release();
     if (pinned) cudaFreeHost(pinned);
     if (h2d_stream) cudaStreamDestroy(h2d_stream);

@@ -88,6 +88,7 @@ struct lsvd_context {
     int64_t launches = 0;
     DeviceBuffer ws_a, ws_u, ws_s, ws_vt, ws_diag, ws_misc, ws_rot, ws_polar;
     DeviceBuffer ws_large;  // large SVD: A, the [G; V] panel store, Gram partials, rotations
+    DeviceBuffer ws_splitk;  // lsvd_gemm_f64: per-slice partial products of a split inner dimension
     // copy streams of the pipelined host-pointer batched path, created on first use
     cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
     // side branch of the large solve's sweep graph (V's update), created on first use

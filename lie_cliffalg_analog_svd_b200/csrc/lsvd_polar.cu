@@ -342,6 +342,21 @@ extern "C" lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N
     return LSVD_OK;
 }
 
+// C = alpha * (sum over z < parts of W[z], each M x N with row stride N) + beta C,
+// one thread per element (consecutive threads on consecutive columns).
+__global__ void splitk_reduce_kernel(const double* __restrict__ W, int parts, int64_t M, int64_t N, double alpha,
+                                     double beta, double* __restrict__ C, int64_t ldc) {
+    const int64_t mn = M * N;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < mn; i += int64_t(gridDim.x) * blockDim.x) {
+        double s = 0.0;
+        for (int z = 0; z < parts; ++z) s += W[z * mn + i];
+        const int64_t r = i / N;
+        double* c = C + r * ldc + (i - r * N);
+        const double v = alpha * s;
+        *c = beta == 0.0 ? v : v + beta * *c;
+    }
+}
+
 extern "C" lsvd_status lsvd_gemm_f64(lsvd_context* ctx, int32_t trans_a, int32_t trans_b, int64_t M,
                                      int64_t N, int64_t K, double alpha, const double* A, int64_t lda,
                                      const double* B, int64_t ldb, double beta, double* C, int64_t ldc) {
@@ -354,6 +369,31 @@ extern "C" lsvd_status lsvd_gemm_f64(lsvd_context* ctx, int32_t trans_a, int32_t
     if ((lda | ldb) & 1 || (reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15)
         return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "lsvd_gemm_f64: lda, ldb even and A, B 16-byte aligned");
     cudaSetDevice(ctx->device);
+    // Few output tiles over a long inner dimension (a Gram or covariance of a
+    // few rows over many samples): one CTA per tile would walk all of K alone.
+    // Split K into S even slices run as one batched launch into the context's
+    // workspace (slice z reads A and B from column / row z * Kc on), the
+    // remainder as one more product, then C = alpha * (sum of the partials) + beta C.
+    const int64_t tiles = ((M + 127) / 128) * ((N + 63) / 64);
+    const int64_t S = std::min<int64_t>(2 * ctx->num_sms / std::max<int64_t>(tiles, 1), K / 2048);
+    if (S >= 2 && M > 0 && N > 0) {
+        const int64_t Kc = (K / S) & ~int64_t(1), Kr = K - S * Kc, mn = M * N;
+        const int parts = int(S + (Kr > 0 ? 1 : 0));
+        cudaError_t e = cudaSuccess;
+        double* W = static_cast<double*>(ctx->ws_splitk.get(size_t(parts) * size_t(mn) * 8, &e));
+        if (!W) return lsvd_ctx_cuda(ctx, e, "lsvd_gemm_f64: split-K workspace");
+        const int64_t sA = trans_a ? Kc * lda : Kc, sB = trans_b ? Kc : Kc * ldb;
+        e = lsvd::dg::dgemm(ctx->stream, trans_a != 0, trans_b != 0, int(M), int(N), int(Kc), 1.0, A, lda, B, ldb,
+                            0.0, W, N, int(S), sA, sB, mn);
+        if (e == cudaSuccess && Kr > 0)
+            e = lsvd::dg::dgemm(ctx->stream, trans_a != 0, trans_b != 0, int(M), int(N), int(Kr), 1.0,
+                                A + S * sA, lda, B + S * sB, ldb, 0.0, W + S * mn, N);
+        if (e != cudaSuccess) return lsvd_ctx_cuda(ctx, e, "lsvd_gemm_f64: split-K slices");
+        const int blocks = int(std::min<int64_t>((mn + 255) / 256, 4 * int64_t(ctx->num_sms)));
+        splitk_reduce_kernel<<<blocks, 256, 0, ctx->stream>>>(W, parts, M, N, alpha, beta, C, ldc);
+        ctx->launches += 2 + (Kr > 0 ? 1 : 0);
+        return lsvd_ctx_cuda(ctx, cudaGetLastError(), "lsvd_gemm_f64: split-K reduction");
+    }
     cudaError_t e = lsvd::dg::dgemm(ctx->stream, trans_a != 0, trans_b != 0, int(M), int(N), int(K), alpha, A,
                                     lda, B, ldb, beta, C, ldc);
     ctx->launches += 1;

@@ -243,3 +243,17 @@ def adjoint_workload(count: int, m: int, n: int, seed: int, gap: float = 1e-3,
         a[t] = (q1 * s[None, :]) @ q2.T
         sig[t] = s
     return a, sig
+
+
+def bss_workload(channels: int, samples: int, seed: int, noise: float = 0.05):
+    """Phase-BSS input: one sinusoid per source at 0.03 .. 0.43 cycles per
+    sample (distinct lagged autocorrelations), plus Gaussian noise, mixed by
+    I + 0.1 G.  Returns (sources, mixing, observations = mixing @ sources)."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(samples, dtype=np.float64)
+    src = np.empty((channels, samples))
+    for k in range(channels):
+        src[k] = np.sin(2 * np.pi * (0.03 + 0.4 * k / channels) * t + k) * (1 + 0.1 * k)
+    src += noise * rng.standard_normal(src.shape)
+    mix = np.eye(channels) + 0.1 * rng.standard_normal((channels, channels))
+    return src, mix, mix @ src
