@@ -14,6 +14,7 @@ bookkeeping.  The reference's evaluation helpers (``channel_phase_coherence``,
 ``estimate_sir_db``) are also provided for host arrays."""
 from __future__ import annotations
 
+import threading
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -40,6 +41,43 @@ def _to_dev(a: np.ndarray, device):
 
 def _host(t) -> np.ndarray:
     return np.ascontiguousarray(t.cpu().numpy())
+
+
+_tls = threading.local()
+
+
+def _staging(elems: int):
+    """This thread's grow-only page-locked float64 staging buffer (torch CPU
+    tensor) of at least ``elems`` elements: large copies go host array ->
+    staging -> device (and back) at DMA speed instead of through pageable memory."""
+    import torch
+    buf = getattr(_tls, "staging", None)
+    if buf is None or buf.numel() < elems:
+        buf = _tls.staging = None
+        buf = _tls.staging = torch.empty(max(elems, 1), dtype=torch.float64, pin_memory=True)
+    return buf
+
+
+def _to_dev_staged(a: np.ndarray, device):
+    """``_to_dev`` of a large host array through the staging buffer."""
+    import torch
+    rows, cols = a.shape
+    st = _staging(a.size)[:a.size]
+    np.copyto(st.numpy().reshape(rows, cols), a)
+    t = _even(rows, cols, device)
+    t.copy_(st.view(rows, cols), non_blocking=True)
+    torch.cuda.current_stream(device).synchronize()
+    return t
+
+
+def _host_staged(t) -> np.ndarray:
+    """``_host`` of a large device view through the staging buffer."""
+    import torch
+    rows, cols = t.shape
+    st = _staging(rows * cols)[:rows * cols].view(rows, cols)
+    st.copy_(t, non_blocking=True)
+    torch.cuda.current_stream(t.device).synchronize()
+    return st.numpy().copy()
 
 
 def _device(ctx: Context):
@@ -148,7 +186,7 @@ class LieSvdBss:
         ch, s = x.shape
         params = params or PhaseBssParams.for_channels(ch)
         dev = _device(ctx)
-        X = _to_dev(x, dev)
+        X = _to_dev_staged(x, dev)
         # channel means (X 1 / T) and X <- X - mean 1^T, both on the product kernel
         # (the inner dimension padded to 2 with a zero column / row)
         one_col, one_row = _even(s, 2, dev), _even(2, s, dev)
@@ -178,7 +216,7 @@ class LieSvdBss:
         Sep = gemm_f64(V, Wh, trans_a=True, c=_even(ch, s, dev), ctx=ctx)
         unmix = _host(gemm_f64(V, W, trans_a=True, c=_even(ch, ch, dev), ctx=ctx))
         coh = _coherence_on_device(Sep, ctx)
-        sep = _host(Sep)
+        sep = _host_staged(Sep)
         return PhaseBssResult(unmix, sep, coh,
                               PhaseBssTrace(ch, s, floor, tr.initial_offdiag, tr.final_offdiag, tr.rotations,
                                             float(coh.sum() / max(len(coh), 1))))
