@@ -1129,7 +1129,8 @@ def _bss_cpu_sample(args, samples=1 << 17):
     return {"value": samples / el, "unit": "samples/s", "cores": 1, "kind": "port",
             "sample": f"one separation of {BSS_CHANNELS} channels x {samples} samples of the same generator, "
                       f"{el:.2f} s (oracle/oracle_consumers.py: the reference's per-sample lagged-covariance "
-                      "loop, products in ndarray order)"}
+                      "loop compiled in oracle/lsvd_oracle.cpp, products in ndarray order, 1 thread as the "
+                      "reference runs it)"}
 
 
 def run_reference_bss(args):

@@ -937,6 +937,25 @@ int oracle_dot(int64_t m, int64_t k, int64_t n, const double* A, const double* B
     return 0;
 }
 
+// One lagged covariance of Phase-BSS (src/lie_svd_bss.rs:172-190): for t
+// ascending, then i, then j, C[i][j] += x[i][t + lag] * x[j][t] / (T - lag),
+// each product divided before it is added; then C <- (C + C^T) / 2
+// (src/lie_svd_bss.rs:187, ndarray's 0.5 * (&c + &c.t())).
+int oracle_lagged_covariance(int64_t ch, int64_t samples, const double* x, int64_t lag, double* out) {
+    if (ch < 1 || samples < 2 || lag < 1 || lag >= samples || !x || !out) return -1;
+    const double denom = double(samples - lag);
+    std::vector<double> c(size_t(ch * ch), 0.0);
+    for (int64_t t = 0; t < samples - lag; ++t)
+        for (int64_t i = 0; i < ch; ++i) {
+            const double xi = x[i * samples + t + lag];
+            double* ci = c.data() + i * ch;
+            for (int64_t j = 0; j < ch; ++j) ci[j] += xi * x[j * samples + t] / denom;
+        }
+    for (int64_t i = 0; i < ch; ++i)
+        for (int64_t j = 0; j < ch; ++j) out[i * ch + j] = 0.5 * (c[size_t(i * ch + j)] + c[size_t(j * ch + i)]);
+    return 0;
+}
+
 int oracle_fmt_e17(double x, char* buf, int64_t cap) {
     char tmp[64];
     std::string s;

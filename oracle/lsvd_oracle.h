@@ -129,6 +129,10 @@ void oracle_set_dot_fma(int32_t on);
  * order: sequential fused multiply-adds over k. */
 int oracle_dot(int64_t m, int64_t k, int64_t n, const double* A, const double* B, double* C);
 
+/* One symmetrised lagged covariance of Phase-BSS (src/lie_svd_bss.rs:172-190)
+ * of the ch x samples row-major signal x, in the reference's loop order. */
+int oracle_lagged_covariance(int64_t ch, int64_t samples, const double* x, int64_t lag, double* out);
+
 int oracle_fmt_e17(double x, char* buf, int64_t cap);
 
 #ifdef __cplusplus

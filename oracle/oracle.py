@@ -68,6 +68,7 @@ def lib():
         _lib.oracle_svd_batch.restype = C.c_int64
         _lib.oracle_svd_batch.argtypes = [C.c_int64, V, V, V, V, V, V, V, V, C.c_int32]
         _lib.oracle_dot.argtypes = [C.c_int64, C.c_int64, C.c_int64, P, P, P]
+        _lib.oracle_lagged_covariance.argtypes = [C.c_int64, C.c_int64, P, C.c_int64, P]
     return _lib
 
 
@@ -304,6 +305,16 @@ def dot(a, b) -> np.ndarray:
     c = np.empty((m, n))
     assert lib().oracle_dot(C.c_int64(m), C.c_int64(k), C.c_int64(n), _p(a), _p(b), _p(c)) == 0
     return c
+
+
+def lagged_covariance(x, lag: int) -> np.ndarray:
+    """One symmetrised lagged covariance of Phase-BSS (src/lie_svd_bss.rs:172-190)
+    in the reference's loop order (t, i, j; each product divided, then added)."""
+    x = _c(x)
+    ch, s = x.shape
+    out = np.empty((ch, ch))
+    assert lib().oracle_lagged_covariance(C.c_int64(ch), C.c_int64(s), _p(x), C.c_int64(lag), _p(out)) == 0
+    return out
 
 
 def _next_centered(state: list) -> float:

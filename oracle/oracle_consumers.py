@@ -6,8 +6,9 @@ TEST INFRASTRUCTURE ONLY, like the rest of ``oracle/``: the checker for
 ``lie_cliffalg_analog_svd_b200.consumers``.  Every step follows the reference
 in its own order: the solves are the oracle's ``LieSvdSmall`` /
 ``LieSvdJoint`` (C++ restatements), the products the oracle's ``dot``
-(ndarray's sequential product order), the per-entry loops numpy statements
-with the same operation order per entry."""
+(ndarray's sequential product order), the lagged covariances the C++ loop
+``oracle_lagged_covariance`` (the reference's t, i, j order), the other
+per-entry loops numpy statements with the same operation order per entry."""
 from __future__ import annotations
 
 from dataclasses import dataclass, field
@@ -61,17 +62,15 @@ def center_channels(x):
 
 def lagged_covariances(x, lags):
     """src/lie_svd_bss.rs:172-195: per lag, C += x[:, t+lag] x[:, t]^T / (T - lag)
-    term by term (each product divided, then added), symmetrised."""
+    term by term (each product divided, then added), symmetrised -- the C++
+    oracle's loop in the reference's order; lags 0 and >= T are skipped, and
+    with none left the plain covariance x x^T / T stands in."""
     ch, t_len = x.shape
     out = []
     for lag in lags:
         if lag == 0 or lag >= t_len:
             continue
-        denom = float(t_len - lag)
-        c = np.zeros((ch, ch))
-        for t in range(t_len - lag):
-            c += np.outer(x[:, t + lag], x[:, t]) / denom
-        out.append(0.5 * (c + c.T))
+        out.append(O.lagged_covariance(x, lag))
     if not out:
         out.append(O.dot(x, x.T.copy()) / t_len)
     return out
