@@ -34,3 +34,14 @@ def test_small_route_model_is_the_reference_count():
     got = b.flops_per_matrix(n, it, sw, rot, np.ones(200, dtype=int))
     want = reference_flops(n.astype(float), it, sw, rot)
     assert np.allclose(got, want, rtol=0, atol=0)
+
+
+def test_bss_model_counts_the_products_of_a_separation():
+    # src/lie_svd_bss.rs:57-100: covariance, whitening and separation (2 C^2 T each), one lagged
+    # covariance per kept lag (2 C^2 (T - lag)); the channel means and the centring update are
+    # products with an inner dimension of 2 (4 C T each)
+    b = _bench()
+    ch, s = 32, 1000
+    lags = [0, 1, 2, 3, 5, 1000, 2000]  # lag 0 and lags >= T are skipped
+    want = 3 * 2 * ch * ch * s + sum(2 * ch * ch * (s - g) for g in (1, 2, 3, 5)) + 2 * 4 * ch * s
+    assert b.bss_flops(ch, s, lags) == want
