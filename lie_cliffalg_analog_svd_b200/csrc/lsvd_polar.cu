@@ -357,6 +357,62 @@ __global__ void splitk_reduce_kernel(const double* __restrict__ W, int parts, in
     }
 }
 
+// Partial products C_z = A_z B_z^T of a split inner dimension for small outputs
+// (M, N <= 16 T; A row-major M x K, B row-major N x K): CTA z accumulates the K
+// columns [z Kc, min(K, (z + 1) Kc)) with CUDA-core FMAs -- an M x N output on
+// 128-wide tensor tiles would waste most of each tile -- and writes its M x N
+// partial to W + z M N (row stride N).  256 threads as 16 x 16, each owning a
+// T x T block of C; slices of 32 columns staged k-major in shared memory so
+// that a warp's reads of A broadcast and its reads of B are consecutive.
+template <int T>
+__global__ void __launch_bounds__(256) gram_slices_kernel(const double* __restrict__ A, int64_t lda,
+                                                          const double* __restrict__ B, int64_t ldb, int M, int N,
+                                                          int64_t K, int64_t Kc, double* __restrict__ W) {
+    constexpr int BK = 32, R = 16 * T;
+    __shared__ double As[BK][R + 1];
+    __shared__ double Bs[BK][R + 1];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int64_t k0 = int64_t(blockIdx.x) * Kc, k1 = k0 + Kc < K ? k0 + Kc : K;
+    const int rows = M > N ? M : N;
+    double acc[T][T];
+#pragma unroll
+    for (int i = 0; i < T; ++i)
+#pragma unroll
+        for (int j = 0; j < T; ++j) acc[i][j] = 0.0;
+    for (int64_t kb = k0; kb < k1; kb += BK) {
+        for (int e = tid; e < rows * BK; e += 256) {
+            const int r = e / BK, c = e - r * BK;  // a warp reads 32 consecutive columns of one row
+            const int64_t k = kb + c;
+            As[c][r] = (r < M && k < k1) ? A[r * lda + k] : 0.0;
+            Bs[c][r] = (r < N && k < k1) ? B[r * ldb + k] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int c = 0; c < BK; ++c) {
+            double a[T], b[T];
+#pragma unroll
+            for (int i = 0; i < T; ++i) a[i] = As[c][ty * T + i];
+#pragma unroll
+            for (int j = 0; j < T; ++j) b[j] = Bs[c][tx * T + j];
+#pragma unroll
+            for (int i = 0; i < T; ++i)
+#pragma unroll
+                for (int j = 0; j < T; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+    double* Wz = W + int64_t(blockIdx.x) * M * N;
+#pragma unroll
+    for (int i = 0; i < T; ++i) {
+        const int r = ty * T + i;
+#pragma unroll
+        for (int j = 0; j < T; ++j) {
+            const int c = tx * T + j;
+            if (r < M && c < N) Wz[int64_t(r) * N + c] = acc[i][j];
+        }
+    }
+}
+
 extern "C" lsvd_status lsvd_gemm_f64(lsvd_context* ctx, int32_t trans_a, int32_t trans_b, int64_t M,
                                      int64_t N, int64_t K, double alpha, const double* A, int64_t lda,
                                      const double* B, int64_t ldb, double beta, double* C, int64_t ldc) {
@@ -369,6 +425,28 @@ extern "C" lsvd_status lsvd_gemm_f64(lsvd_context* ctx, int32_t trans_a, int32_t
     if ((lda | ldb) & 1 || (reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15)
         return lsvd_ctx_fail(ctx, LSVD_UNSUPPORTED, "lsvd_gemm_f64: lda, ldb even and A, B 16-byte aligned");
     cudaSetDevice(ctx->device);
+    // A B^T with both output dimensions <= 64 over a long inner dimension (a
+    // covariance of a few channels over many samples): CUDA-core slices of at
+    // least 1024 columns, up to four per SM, then the reduction below.
+    if (!trans_a && trans_b && M > 0 && N > 0 && M <= 64 && N <= 64 && K >= 4096) {
+        const int64_t S = std::min<int64_t>(4 * int64_t(ctx->num_sms), (K + 1023) / 1024);
+        const int64_t Kc = (K + S - 1) / S, parts = (K + Kc - 1) / Kc, mn = M * N;
+        cudaError_t e = cudaSuccess;
+        double* W = static_cast<double*>(ctx->ws_splitk.get(size_t(parts) * size_t(mn) * 8, &e));
+        if (!W) return lsvd_ctx_cuda(ctx, e, "lsvd_gemm_f64: split-K workspace");
+        const int mx = int(std::max(M, N));
+        const unsigned g = unsigned(parts);
+        if (mx <= 16)
+            gram_slices_kernel<1><<<g, 256, 0, ctx->stream>>>(A, lda, B, ldb, int(M), int(N), K, Kc, W);
+        else if (mx <= 32)
+            gram_slices_kernel<2><<<g, 256, 0, ctx->stream>>>(A, lda, B, ldb, int(M), int(N), K, Kc, W);
+        else
+            gram_slices_kernel<4><<<g, 256, 0, ctx->stream>>>(A, lda, B, ldb, int(M), int(N), K, Kc, W);
+        const int blocks = int(std::min<int64_t>((mn + 255) / 256, 4 * int64_t(ctx->num_sms)));
+        splitk_reduce_kernel<<<blocks, 256, 0, ctx->stream>>>(W, int(parts), M, N, alpha, beta, C, ldc);
+        ctx->launches += 2;
+        return lsvd_ctx_cuda(ctx, cudaGetLastError(), "lsvd_gemm_f64: small-output slices");
+    }
     // Few output tiles over a long inner dimension (a Gram or covariance of a
     // few rows over many samples): one CTA per tile would walk all of K alone.
     // Split K into S even slices run as one batched launch into the context's

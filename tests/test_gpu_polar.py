@@ -45,11 +45,13 @@ def _round_bf16(x: np.ndarray) -> np.ndarray:
 @pytest.mark.parametrize("ta,tb", [(False, False), (True, False), (False, True), (True, True)])
 @pytest.mark.parametrize("M,N,K", [(128, 128, 16), (1, 1, 1), (7, 9, 5), (130, 257, 33), (300, 200, 1000),
                                    (512, 384, 4096), (64, 1000, 3), (2560, 2312, 96),
-                                   (32, 32, 300001), (5, 70, 65537), (130, 64, 100000)])
+                                   (32, 32, 300001), (5, 70, 65537), (130, 64, 100000),
+                                   (64, 64, 50001), (3, 17, 9000), (16, 9, 4096)])
 def test_gemm_f64(ta, tb, M, N, K):
     # the small shapes run on 128 x 64 tiles, (2560, 2312, 96) on 128 x 128 tiles;
-    # the last three split K into slices (few output tiles, K >= 4096; odd K
-    # leaves a remainder slice)
+    # the last six split K into slices (few output tiles, K >= 4096; odd K
+    # leaves a remainder slice); A B^T with M, N <= 64 takes the CUDA-core
+    # slices (T = 4, 2, 2, 1 for the 64, 32, 17 and 16 wide outputs)
     import torch
     rng = np.random.default_rng(M * 13 + N * 5 + K + 2 * ta + tb)
     a = rng.standard_normal((K, M) if ta else (M, K))
