@@ -362,31 +362,45 @@ __global__ void splitk_reduce_kernel(const double* __restrict__ W, int parts, in
 // columns [z Kc, min(K, (z + 1) Kc)) with CUDA-core FMAs -- an M x N output on
 // 128-wide tensor tiles would waste most of each tile -- and writes its M x N
 // partial to W + z M N (row stride N).  256 threads as 16 x 16, each owning a
-// T x T block of C; slices of 32 columns staged k-major in shared memory so
-// that a warp's reads of A broadcast and its reads of B are consecutive.
+// T x T block of C.  Slabs of BK = 2048 / (16 T) columns are staged k-major in
+// shared memory (a warp's reads of A broadcast, its reads of B are
+// consecutive); each thread holds its 8 + 8 elements of the next slab in
+// registers while the current slab is multiplied.
 template <int T>
 __global__ void __launch_bounds__(256) gram_slices_kernel(const double* __restrict__ A, int64_t lda,
                                                           const double* __restrict__ B, int64_t ldb, int M, int N,
                                                           int64_t K, int64_t Kc, double* __restrict__ W) {
-    constexpr int BK = 32, R = 16 * T;
+    constexpr int R = 16 * T, BK = 2048 / R, PER = R * BK / 256;  // PER = 8
+    static_assert(BK >= 32 && PER * 256 == R * BK, "slab shape");
     __shared__ double As[BK][R + 1];
     __shared__ double Bs[BK][R + 1];
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     const int64_t k0 = int64_t(blockIdx.x) * Kc, k1 = k0 + Kc < K ? k0 + Kc : K;
-    const int rows = M > N ? M : N;
     double acc[T][T];
 #pragma unroll
     for (int i = 0; i < T; ++i)
 #pragma unroll
         for (int j = 0; j < T; ++j) acc[i][j] = 0.0;
-    for (int64_t kb = k0; kb < k1; kb += BK) {
-        for (int e = tid; e < rows * BK; e += 256) {
-            const int r = e / BK, c = e - r * BK;  // a warp reads 32 consecutive columns of one row
+    double ra[PER], rb[PER];
+    auto fetch = [&](int64_t kb) {
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int e = tid + 256 * q, r = e / BK, c = e - r * BK;  // a warp: 32 consecutive columns of a row
             const int64_t k = kb + c;
-            As[c][r] = (r < M && k < k1) ? A[r * lda + k] : 0.0;
-            Bs[c][r] = (r < N && k < k1) ? B[r * ldb + k] : 0.0;
+            ra[q] = (r < M && k < k1) ? A[r * lda + k] : 0.0;
+            rb[q] = (r < N && k < k1) ? B[r * ldb + k] : 0.0;
+        }
+    };
+    fetch(k0);
+    for (int64_t kb = k0; kb < k1; kb += BK) {
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int e = tid + 256 * q, r = e / BK, c = e - r * BK;
+            As[c][r] = ra[q];
+            Bs[c][r] = rb[q];
         }
         __syncthreads();
+        if (kb + BK < k1) fetch(kb + BK);
 #pragma unroll 8
         for (int c = 0; c < BK; ++c) {
             double a[T], b[T];
