@@ -187,13 +187,13 @@ class LieSvdBss:
         params = params or PhaseBssParams.for_channels(ch)
         dev = _device(ctx)
         X = _to_dev_staged(x, dev)
-        # channel means (X 1 / T) and X <- X - mean 1^T, both on the product kernel
-        # (the inner dimension padded to 2 with a zero column / row)
-        one_col, one_row = _even(s, 2, dev), _even(2, s, dev)
-        one_col[:, 0] = 1.0
-        one_row[0, :] = 1.0
-        mean = gemm_f64(X, one_col, alpha=1.0 / s, c=_even(ch, 2, dev), ctx=ctx)
-        gemm_f64(mean, one_row, alpha=-1.0, beta=1.0, c=X, ctx=ctx)
+        # channel means (X 1 / T, as X E^T with E = [1^T; 0^T]: a narrow output over
+        # the long sample axis) and X <- X - mean 1^T (E again, the inner
+        # dimension padded to 2), both on the product kernel
+        ones = _even(2, s, dev)
+        ones[0, :] = 1.0
+        mean = gemm_f64(X, ones, trans_b=True, alpha=1.0 / s, c=_even(ch, 2, dev), ctx=ctx)
+        gemm_f64(mean, ones, alpha=-1.0, beta=1.0, c=X, ctx=ctx)
         cov = _host(gemm_f64(X, X, trans_b=True, alpha=1.0 / s, c=_even(ch, ch, dev), ctx=ctx))
         u, sigma, _ = LieSvdSmall.solve(cov, ctx=ctx)
         floor = params.eps * max(float(np.max(sigma)), 0.0, 1.0)
