@@ -59,10 +59,13 @@ def test_bss_reference_test_through_the_gpu():  # src/lie_svd_bss.rs:216-251
     assert np.isfinite(g.trace.mean_channel_coherence)
 
 
-@pytest.mark.parametrize("channels,samples,lags", [(3, 6, [0, 7]), (5, 1001, [1, 2, 3, 5]), (16, 4099, [1, 4, 9])])
+@pytest.mark.parametrize("channels,samples,lags", [(3, 6, [0, 7]), (5, 1001, [1, 2, 3, 5]), (16, 4099, [1, 4, 9]),
+                                                   (80, 6000, [1, 2, 3, 5])])
 def test_bss_shapes_and_lags(channels, samples, lags):
     # odd sample counts (ragged rows on the product kernel), lags beyond the
-    # samples (the covariance fallback) and more channels than the reference test
+    # samples (the covariance fallback) and more channels than the reference test;
+    # 80 channels take the large solve for the covariance SVD and the tensor-tile
+    # split-K products (outputs wider than 64)
     rng = np.random.default_rng(channels)
     t = np.arange(samples, dtype=np.float64)
     # one sinusoid per channel at 0.03 .. 0.43 cycles per sample: well-separated
