@@ -58,26 +58,49 @@ def _staging(elems: int):
     return buf
 
 
+_STAGE_CHUNKS = 8
+
+
+def _row_chunks(rows: int):
+    step = max(1, -(-rows // _STAGE_CHUNKS))
+    return [(r, min(rows, r + step)) for r in range(0, rows, step)]
+
+
 def _to_dev_staged(a: np.ndarray, device):
-    """``_to_dev`` of a large host array through the staging buffer."""
+    """``_to_dev`` of a large host array through the staging buffer, in row
+    chunks: the DMA of one chunk runs while the host copies the next one into
+    its own part of the staging buffer."""
     import torch
     rows, cols = a.shape
-    st = _staging(a.size)[:a.size]
-    np.copyto(st.numpy().reshape(rows, cols), a)
+    st = _staging(a.size)[:a.size].view(rows, cols)
+    sn = st.numpy()
     t = _even(rows, cols, device)
-    t.copy_(st.view(rows, cols), non_blocking=True)
+    for r0, r1 in _row_chunks(rows):
+        np.copyto(sn[r0:r1], a[r0:r1])
+        t[r0:r1].copy_(st[r0:r1], non_blocking=True)
     torch.cuda.current_stream(device).synchronize()
     return t
 
 
 def _host_staged(t) -> np.ndarray:
-    """``_host`` of a large device view through the staging buffer."""
+    """``_host`` of a large device view through the staging buffer, in row
+    chunks: the host copies one chunk out while the DMA of the next one runs."""
     import torch
     rows, cols = t.shape
     st = _staging(rows * cols)[:rows * cols].view(rows, cols)
-    st.copy_(t, non_blocking=True)
-    torch.cuda.current_stream(t.device).synchronize()
-    return st.numpy().copy()
+    sn = st.numpy()
+    out = np.empty((rows, cols))
+    stream = torch.cuda.current_stream(t.device)
+    done = []
+    for r0, r1 in _row_chunks(rows):
+        st[r0:r1].copy_(t[r0:r1], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        done.append((r0, r1, ev))
+    for r0, r1, ev in done:
+        ev.synchronize()
+        np.copyto(out[r0:r1], sn[r0:r1])
+    return out
 
 
 def _device(ctx: Context):
