@@ -375,9 +375,14 @@ LSVD_API lsvd_status lsvd_gemm_nt_lowp(lsvd_context* ctx, int64_t M, int64_t N, 
 /* C = alpha op(A) op(B) + beta C in FP64 (row-major; op(X) = X^T when
  * trans_x != 0) on the FP64 tensor path (mma.sync m8n8k4): the product
  * kernel of the FP64 polar iteration and of the large SVD (the reference's
- * ndarray .dot, src/lie_svd_small.rs:172-173, :305, :313), exposed for
- * testing.  Device pointers; lda, ldb even and A, B 16-byte aligned;
- * enqueued on the context's stream without synchronising. */
+ * ndarray .dot, src/lie_svd_small.rs:172-173, :305, :313), also the
+ * products of the Phase-BSS and canonical-order consumers
+ * (src/lie_svd_bss.rs:64, :74, :81-82, :179-186; src/phase_normalizer.rs:109, :140).
+ * Few output tiles over K >= 4096 split K across the SMs into partials in the
+ * context's workspace, reduced in a second launch (A B^T with M, N <= 64 on
+ * CUDA-core slices, larger outputs as batched tensor-core slices).  Device
+ * pointers; lda, ldb even and A, B 16-byte aligned; enqueued on the
+ * context's stream without synchronising. */
 LSVD_API lsvd_status lsvd_gemm_f64(lsvd_context* ctx, int32_t trans_a, int32_t trans_b, int64_t M,
                                    int64_t N, int64_t K, double alpha, const double* A, int64_t lda,
                                    const double* B, int64_t ldb, double beta, double* C, int64_t ldc);
