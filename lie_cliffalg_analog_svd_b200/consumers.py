@@ -14,6 +14,7 @@ bookkeeping.  The reference's evaluation helpers (``channel_phase_coherence``,
 ``estimate_sir_db``) are also provided for host arrays."""
 from __future__ import annotations
 
+import os
 import threading
 from dataclasses import dataclass, field
 
@@ -59,6 +60,19 @@ def _staging(elems: int):
 
 
 _STAGE_CHUNKS = 8
+_copy_pool = None
+_copy_pool_lock = threading.Lock()
+
+
+def _copier():
+    """Process-wide thread pool for the host side of the staged copies
+    (numpy's copy releases the GIL, so the chunks copy in parallel)."""
+    global _copy_pool
+    with _copy_pool_lock:
+        if _copy_pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            _copy_pool = ThreadPoolExecutor(max_workers=max(1, min(_STAGE_CHUNKS, os.cpu_count() or 1)))
+        return _copy_pool
 
 
 def _row_chunks(rows: int):
@@ -68,15 +82,17 @@ def _row_chunks(rows: int):
 
 def _to_dev_staged(a: np.ndarray, device):
     """``_to_dev`` of a large host array through the staging buffer, in row
-    chunks: the DMA of one chunk runs while the host copies the next one into
-    its own part of the staging buffer."""
+    chunks copied into it by a thread pool; each chunk's DMA is issued as soon
+    as its host copy is done, beside the copies still running."""
     import torch
     rows, cols = a.shape
     st = _staging(a.size)[:a.size].view(rows, cols)
     sn = st.numpy()
     t = _even(rows, cols, device)
-    for r0, r1 in _row_chunks(rows):
-        np.copyto(sn[r0:r1], a[r0:r1])
+    chunks = _row_chunks(rows)
+    jobs = [_copier().submit(np.copyto, sn[r0:r1], a[r0:r1]) for r0, r1 in chunks]
+    for (r0, r1), job in zip(chunks, jobs):
+        job.result()
         t[r0:r1].copy_(st[r0:r1], non_blocking=True)
     torch.cuda.current_stream(device).synchronize()
     return t
@@ -84,7 +100,8 @@ def _to_dev_staged(a: np.ndarray, device):
 
 def _host_staged(t) -> np.ndarray:
     """``_host`` of a large device view through the staging buffer, in row
-    chunks: the host copies one chunk out while the DMA of the next one runs."""
+    chunks: every chunk's DMA is enqueued at once, and each is copied out by
+    the thread pool as soon as its event has completed."""
     import torch
     rows, cols = t.shape
     st = _staging(rows * cols)[:rows * cols].view(rows, cols)
@@ -97,9 +114,12 @@ def _host_staged(t) -> np.ndarray:
         ev = torch.cuda.Event()
         ev.record(stream)
         done.append((r0, r1, ev))
+    jobs = []
     for r0, r1, ev in done:
         ev.synchronize()
-        np.copyto(out[r0:r1], sn[r0:r1])
+        jobs.append(_copier().submit(np.copyto, out[r0:r1], sn[r0:r1]))
+    for job in jobs:
+        job.result()
     return out
 
 
