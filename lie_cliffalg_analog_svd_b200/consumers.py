@@ -86,7 +86,10 @@ def _to_dev_staged(a: np.ndarray, device):
     as its host copy is done, beside the copies still running."""
     import torch
     rows, cols = a.shape
-    st = _staging(a.size)[:a.size].view(rows, cols)
+    try:
+        st = _staging(a.size)[:a.size].view(rows, cols)
+    except RuntimeError:  # page-locked memory exhausted: copy straight from the pageable array
+        return _to_dev(a, device)
     sn = st.numpy()
     t = _even(rows, cols, device)
     chunks = _row_chunks(rows)
@@ -104,7 +107,10 @@ def _host_staged(t) -> np.ndarray:
     the thread pool as soon as its event has completed."""
     import torch
     rows, cols = t.shape
-    st = _staging(rows * cols)[:rows * cols].view(rows, cols)
+    try:
+        st = _staging(rows * cols)[:rows * cols].view(rows, cols)
+    except RuntimeError:  # page-locked memory exhausted: copy straight into pageable memory
+        return _host(t)
     sn = st.numpy()
     out = np.empty((rows, cols))
     stream = torch.cuda.current_stream(t.device)
