@@ -139,6 +139,14 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_for(self, count: int, timeout: float = 2.0):
+        """Block until ``count`` samples have arrived (bounded), so that a
+        timed region shorter than the 200 ms sampling period still has a
+        sample at each end."""
+        end = time.perf_counter() + timeout
+        while self.proc is not None and len(self.lines) < count and time.perf_counter() < end:
+            time.sleep(0.01)
+
     def __exit__(self, *a):
         if self.proc:
             self.proc.terminate()
@@ -1087,11 +1095,13 @@ def run_bss(args):
     torch.cuda.synchronize()
     l0 = ctx.kernel_launches
     with ClockSampler(local) as clk:
+        clk.wait_for(1)  # a separation takes tens of ms: sample at both ends of the timed region
         t0 = time.perf_counter()
         for _ in range(args.steps):
             LieSvdBss.separate(obs, params, ctx=ctx)
         torch.cuda.synchronize()
         el = _max_over_ranks(torch, ws, device, (time.perf_counter() - t0) / args.steps)
+        clk.wait_for(len(clk.lines) + 1, 0.5)
     launches = (ctx.kernel_launches - l0) // max(args.steps, 1)
     h2d, d2h = obs.nbytes, obs.nbytes + ch * ch * 8 * (len(BSS_LAGS) + 2)
     line = _base_line(args, "samples/s", ws * s / el, el * 1e3, ws, f"phase_bss_{ch}ch_{s}samples",
